@@ -1,0 +1,146 @@
+/* dwf_b200.h -- C ABI of the B200 (sm_100a) implementation of the lattice
+ * study's dynamical-fermion hot path: the Wilson and domain-wall Dirac
+ * operators, CG on the normal operator, the pseudofermion force and link
+ * update inside HMC, and the propagator solves with their meson contractions.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns an int status (dwf_status). Host layouts are the reference's:
+ *
+ *   gauge theta  double[2*Nt*Nx]          index (mu*Nt + t)*Nx + x
+ *                                           (domain_wall/include/indexing.hpp:10-13,
+ *                                            wilson/include/indexing.hpp:9-12)
+ *   DWF fermion  complex<double>[Ls*Nt*Nx*2], interleaved (re, im),
+ *                index ((s*Nt + t)*Nx + x)*2 + spin  (domain_wall/include/indexing.hpp:5-8)
+ *   Wilson       complex<double>[Nt*Nx*2], index (t*Nx + x)*2 + spin
+ *                                           (wilson/include/indexing.hpp:5-8)
+ *
+ * Entry points whose name ends in _dev take device pointers (laid out the
+ * same way, one right-hand side after another) and run on the context's
+ * stream; the others take host pointers and copy.
+ *
+ * Ownership: the caller owns every buffer it passes. A context owns its
+ * device memory and stream. One context per host thread: a context is not
+ * safe for concurrent use, distinct contexts are independent.
+ */
+#ifndef DWF_B200_H
+#define DWF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The C++ host layer maps them to the reference's
+ * std::runtime_error messages (e.g. "CG encountered a zero denominator",
+ * domain_wall/include/cg_solver.hpp:45-46). */
+typedef enum
+{
+    DWF_OK = 0,
+    DWF_NOT_CONVERGED = 1,
+    DWF_ZERO_DENOM = 2,
+    DWF_NONFINITE = 3,
+    DWF_CUDA_ERROR = 4,
+    DWF_TIMEOUT = 5,
+    DWF_BAD_ARG = 6
+} dwf_status;
+
+/* Operators (domain_wall/include/dwf_operator.hpp:15,94,173,178). */
+typedef enum
+{
+    DWF_OP_D = 0,
+    DWF_OP_DDAG = 1,
+    DWF_OP_DDDAG = 2, /* D D^dag  (pseudofermion solve) */
+    DWF_OP_DDAGD = 3  /* D^dag D  (propagator / CGNR solve) */
+} dwf_op;
+
+/* Solver paths. */
+typedef enum
+{
+    /* The reference algorithm in FP64: unpreconditioned CG, stop when the
+     * recursive residual satisfies |r|/|b| <= rtol
+     * (domain_wall/include/cg_solver.hpp:17-64). */
+    DWF_SOLVER_CG64 = 0,
+    /* FP32 inner CG iterations with FP64 reliable updates (true residual
+     * recomputed in FP64); converged only when the FP64 true residual meets
+     * rtol. Falls back to DWF_SOLVER_CG64 from its current iterate if the
+     * true residual stalls. */
+    DWF_SOLVER_MIXED = 1
+} dwf_solver;
+
+/* Domain-wall context parameters: the parameters.txt keys dwf.Nt, dwf.Nx,
+ * dwf.N5, dwf.M5, dwf.mf, dwf.beta (domain_wall/include/parameters.hpp:7-20). */
+typedef struct
+{
+    int Nt, Nx, Ls;
+    double M5, mf;
+    double beta;
+    int device; /* CUDA device ordinal */
+} dwf_params;
+
+/* Per-solve report. */
+typedef struct
+{
+    int iterations;      /* CG iterations, counted as the reference counts them */
+    int converged;       /* 1 if the stopping rule was met */
+    int status;          /* dwf_status of this right-hand side */
+    int solver;          /* dwf_solver path that produced x */
+    double relres;       /* recursive residual |r|/|b| at exit */
+    double true_relres;  /* FP64 |b - A x| / |b| recomputed after the solve */
+    int reliable_updates;/* FP64 residual replacements (mixed path) */
+    int fallback;        /* 1 if the mixed path fell back to FP64 CG */
+} dwf_solve_info;
+
+typedef struct dwf_ctx dwf_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+int dwf_ctx_create(const dwf_params* params, dwf_ctx** out);
+int dwf_ctx_destroy(dwf_ctx* ctx);
+const char* dwf_status_string(int status);
+/* Last error message recorded on this context ("" if none). */
+const char* dwf_last_error(const dwf_ctx* ctx);
+/* Limit (ns) for every bounded wait inside persistent kernels (default 5 s). */
+int dwf_set_wait_limit(dwf_ctx* ctx, uint64_t nanoseconds);
+/* Synchronise the context stream. */
+int dwf_sync(dwf_ctx* ctx);
+/* The context's cudaStream_t, as void*. */
+void* dwf_stream(dwf_ctx* ctx);
+
+/* ---- gauge field ---------------------------------------------------------- */
+/* Upload nconf configurations (host, nconf * 2*Nt*Nx doubles). The context
+ * caches link phases U = exp(i theta) in FP64 and FP32
+ * (domain_wall/include/dwf_operator.hpp:10-13). */
+int dwf_set_gauge(dwf_ctx* ctx, int nconf, const double* theta);
+/* Same from a device buffer. */
+int dwf_set_gauge_dev(dwf_ctx* ctx, int nconf, const double* theta_dev);
+
+/* ---- operators ---------------------------------------------------------- */
+/* out = op(in) for nrhs fields, all on configuration `conf`
+ * (apply_D / apply_D_dagger / apply_DD_dagger / apply_D_dagger_D,
+ *  domain_wall/include/dwf_operator.hpp:15-181). */
+int dwf_apply(dwf_ctx* ctx, int op, int conf, const double* in, double* out, int nrhs);
+/* Device version; precision 64 (complex<double>) or 32 (complex<float>). */
+int dwf_apply_dev(dwf_ctx* ctx, int op, int conf, const void* in_dev, void* out_dev, int nrhs,
+                  int precision);
+
+/* ---- solver ----------------------------------------------------------------- */
+/* Solve A x = b with A = op (DWF_OP_DDDAG or DWF_OP_DDAGD) on configuration
+ * `conf`. x is read as the initial guess when has_guess != 0 (the reference's
+ * initial_guess pointer), else started from zero. Host pointers.
+ * (conjugate_gradient, domain_wall/include/cg_solver.hpp:17-64) */
+int dwf_cg(dwf_ctx* ctx, int op, int conf, const double* b, double* x, int has_guess,
+           double rtol, int maxiter, int solver, dwf_solve_info* info);
+/* Batched device version: nrhs right-hand sides, rhs k on configuration
+ * rhs_conf[k] (host array; NULL = all on configuration 0), solved together
+ * in one persistent launch with per-right-hand-side convergence.
+ * info: host array of nrhs reports. */
+int dwf_cg_batch_dev(dwf_ctx* ctx, int op, int nrhs, const int* rhs_conf, const void* b_dev,
+                     void* x_dev, int has_guess, double rtol, int maxiter, int solver,
+                     dwf_solve_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DWF_B200_H */

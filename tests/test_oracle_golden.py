@@ -1,0 +1,179 @@
+"""The CPU oracle against golden vectors produced by the reference itself
+(tests/golden/make_golden.py runs the reference's C++ compiled unmodified).
+The oracle restates the reference's arithmetic in the same order, so the
+agreement is exact."""
+import csv
+
+import numpy as np
+import pytest
+
+from conftest import rel
+from oracle import oracle as O
+
+DWF_CASES = ["dwf_8x8x4", "dwf_6x10x3"]
+WIL_CASES = ["wil_8x8", "wil_6x10"]
+
+
+def dwf_of(g):
+    p = g.p
+    return O.Dwf(p["dwf.Nt"], p["dwf.Nx"], p["dwf.N5"], p["dwf.M5"], p["dwf.mf"])
+
+
+@pytest.mark.parametrize("case", DWF_CASES)
+def test_dwf_operators(golden, case):
+    g = golden(case)
+    d = dwf_of(g)
+    th, psi = g.npy("in_theta.npy"), g.field("in_psi.npy")
+    for op, name in [(O.D, "D"), (O.DDAG, "Ddag"), (O.DDDAG, "DDdag"), (O.DDAGD, "DdagD")]:
+        assert rel(d.apply(op, th, psi), g.field(f"out_{name}.npy")) == 0.0
+
+
+@pytest.mark.parametrize("case", DWF_CASES)
+def test_dwf_cg_and_forces(golden, case):
+    g = golden(case)
+    d = dwf_of(g)
+    p = g.p
+    th, psi, chi = g.npy("in_theta.npy"), g.field("in_psi.npy"), g.field("in_chi.npy")
+    x, it, rr, st = d.cg(O.DDAGD, th, d.apply(O.DDAG, th, psi), p["dwf.propagator_rtol"],
+                         p["dwf.propagator_maxiter"])
+    info = g.npy("out_cg_info.npy")
+    assert st == 0 and it == info[0] and rr == info[1]
+    assert rel(x, g.field("out_cg_x.npy")) == 0.0
+    pf = d.pf_action_force(th, d.apply(O.D, th, chi), p["dwf.pseudofermion_rtol"],
+                           p["dwf.pseudofermion_maxiter"])
+    pinfo = g.npy("out_pf_info.npy")
+    assert pf["action"] == pinfo[0] and pf["iterations"] == pinfo[1]
+    assert rel(pf["force"], g.npy("out_pf_force.npy")) == 0.0
+    assert rel(pf["eta"], g.field("out_pf_eta.npy")) == 0.0
+    warm = d.pf_action_force(th, d.apply(O.D, th, chi), p["dwf.pseudofermion_rtol"],
+                             p["dwf.pseudofermion_maxiter"], guess=pf["eta"])
+    assert warm["iterations"] == g.npy("out_pf_warm_info.npy")[1]
+    a, f = O.gauge_action_force(d.Nt, d.Nx, p["dwf.beta"], th)
+    ginfo = g.npy("out_gauge_info.npy")
+    assert a == ginfo[0] and rel(f, g.npy("out_gauge_force.npy")) == 0.0
+    assert O.average_plaquette(d.Nt, d.Nx, th) == ginfo[1]
+
+
+@pytest.mark.parametrize("case", DWF_CASES)
+def test_dwf_measurements(golden, case):
+    g = golden(case)
+    d = dwf_of(g)
+    p = g.p
+    th = g.npy("in_theta.npy")
+    rt, mi = p["dwf.propagator_rtol"], p["dwf.propagator_maxiter"]
+    st, cpp, cj5 = d.cpp_cj5(th, rt, mi)
+    assert st == 0 and rel(cpp, g.npy("out_cpp.npy")) == 0.0
+    assert rel(cj5, g.npy("out_cj5.npy")) == 0.0
+    st, mom = d.momentum_cpp(th, p["analysis.max_momentum"], rt, mi)
+    assert st == 0 and rel(mom, g.npy("out_mom.npy")) == 0.0
+    st, lp = d.loop(th, p["eta.random_seed"], p["eta.noise_vectors"], rt, mi)
+    assert st == 0 and rel(lp, g.field("out_loop.npy")) == 0.0
+
+
+def test_dwf_hmc_chain_matches_reference_generator(golden):
+    """Per-trajectory configurations and decisions of the reference's own
+    generate_domain_wall run (its RNG stream, seed 1234) are reproduced."""
+    g = golden("dwf_hmc_8x8x4")
+    p = g.p
+    d = O.Dwf(p["dwf.Nt"], p["dwf.Nx"], p["dwf.N5"], p["dwf.M5"], p["dwf.mf"])
+    cfg = g.npy("configs.npy")
+    hist = list(csv.DictReader(open(g.dir / "run_info_history.csv")))
+    chi, mom, u = O.dwf_draws(p["dwf.random_seed"], p["dwf.trajectories"], d.ndof, d.ngauge)
+    th = np.ones(d.ngauge)
+    for k in range(p["dwf.trajectories"]):
+        st, prop, inf = d.trajectory(p["dwf.beta"], p["dwf.epsilon"], p["dwf.leapfrog_steps"],
+                                     p["dwf.pseudofermion_rtol"], p["dwf.pseudofermion_maxiter"],
+                                     th, chi[k], mom[k])
+        assert st == 0
+        acc = u[k] < min(np.exp(-inf["dH"]), 1.0)
+        assert int(acc) == int(hist[k]["accepted"])
+        assert float(hist[k]["delta_h"]) == pytest.approx(inf["dH"], rel=1e-5, abs=1e-9)
+        if acc:
+            th = prop
+        assert rel(th, cfg[k].ravel()) == 0.0
+
+
+@pytest.mark.parametrize("case", WIL_CASES)
+def test_wilson(golden, case):
+    g = golden(case)
+    p = g.p
+    w = O.Wilson(p["wilson.Nt"], p["wilson.Nx"], p["wilson.m0"], p["wilson.time_boundary_sign"],
+                 p["wilson.space_boundary_sign"])
+    th, psi = g.npy("in_theta.npy"), g.field("in_psi.npy")
+    assert rel(w.apply(O.D, th, psi), g.field("out_D.npy")) == 0.0
+    assert rel(w.apply(O.DDAG, th, psi), g.field("out_Ddag.npy")) == 0.0
+    st, x, info = w.solve_cgnr(th, psi, p["wilson.measurement_cg_tolerance"],
+                               p["wilson.measurement_cg_max_iterations"])
+    assert st == 0 and np.array_equal(info, g.npy("out_cgnr_info.npy"))
+    assert rel(x, g.field("out_cgnr_x.npy")) == 0.0
+    st, eta, res = w.solve_dddag(th, psi, p["wilson.force_cg_tolerance"],
+                                 p["wilson.force_cg_max_iterations"])
+    assert st == 0 and rel(eta, g.field("out_dddag_x.npy")) == 0.0
+    acts = g.npy("out_actions.npy")
+    a, f = O.gauge_action_force(w.Nt, w.Nx, p["wilson.beta"], th)
+    assert a == acts[0] and rel(f, g.npy("out_gauge_force.npy")) == 0.0
+    st, spf, fpf = w.pf_action_force(th, psi, p["wilson.force_cg_tolerance"],
+                                     p["wilson.force_cg_max_iterations"])
+    assert st == 0 and spf == acts[1] and rel(fpf, g.npy("out_pf_force.npy")) == 0.0
+    st, c = w.correlator(th, p["wilson.source_t"], p["wilson.source_x"],
+                         p["wilson.measurement_cg_tolerance"],
+                         p["wilson.measurement_cg_max_iterations"])
+    assert st == 0 and rel(c, g.npy("out_corr.npy")) == 0.0
+
+
+@pytest.mark.parametrize("case", WIL_CASES)
+def test_wilson_hmc_matches_reference_hmc_step(golden, case):
+    g = golden(case)
+    p = g.p
+    w = O.Wilson(p["wilson.Nt"], p["wilson.Nx"], p["wilson.m0"], p["wilson.time_boundary_sign"],
+                 p["wilson.space_boundary_sign"])
+    mom, chi, u = O.wil_draws(p["wilson.random_seed"], 3, w.ntot, w.ngauge)
+    thetas, info = g.npy("out_hmc_theta.npy"), g.npy("out_hmc_info.npy")
+    cur = g.npy("in_theta.npy").ravel()
+    eps = p["wilson.trajectory_length"] / p["wilson.hmc_steps"]
+    for k in range(3):
+        st, cur, inf = w.hmc_step(p["wilson.beta"], eps, p["wilson.hmc_steps"],
+                                  p["wilson.force_cg_tolerance"],
+                                  p["wilson.force_cg_max_iterations"], cur, mom[k], chi[k], u[k])
+        assert st == 0 and inf["dH"] == info[k, 0] and inf["accepted"] == bool(info[k, 2])
+        assert rel(cur, thetas[k].ravel()) == 0.0
+
+
+def test_rng_streams_known_answers():
+    """libstdc++ streams the reference draws from: mt19937_64(1234) +
+    normal_distribution, and mt19937_64(918273) + uniform_int_distribution(0,3)."""
+    assert O.rng_normals(1234, 2).tolist() == [0.20515413959099182, -0.33619173225969745]
+    assert O.rng_z4(918273, 8).tolist() == [1, 0, 2, 1, 1, 3, 1, 0]
+    chi, mom, u = O.dwf_draws(1234, 1, 1, 0)
+    # Complex(normal, normal): the imaginary argument is drawn first
+    assert chi[0, 0] * np.sqrt(2.0) == pytest.approx(-0.33619173225969745 + 0.20515413959099182j,
+                                                      abs=1e-15)
+
+
+def test_oracle_adjointness_and_free_field():
+    """<a, D b> = <D^dag a, b>; D^dag D is Hermitian positive; at theta = 0
+    the Wilson operator's eigenvalues match the free-field plane waves."""
+    rng = np.random.default_rng(5)
+    d = O.Dwf(6, 4, 3, 1.2, 0.1)
+    th = rng.uniform(-np.pi, np.pi, d.ngauge)
+    a = rng.normal(size=d.ndof) + 1j * rng.normal(size=d.ndof)
+    b = rng.normal(size=d.ndof) + 1j * rng.normal(size=d.ndof)
+    lhs = np.vdot(a, d.apply(O.D, th, b))
+    rhs = np.vdot(d.apply(O.DDAG, th, a), b)
+    assert abs(lhs - rhs) < 1e-12 * abs(lhs)
+    w = O.Wilson(4, 6, 0.2, -1.0, 1.0)
+    th0 = np.zeros(w.ngauge)
+    M = np.stack([w.apply(O.D, th0, e) for e in np.eye(w.ntot)], axis=1)
+    ev = np.sort_complex(np.linalg.eigvals(M))
+    expect = []
+    for nt in range(4):
+        for nx in range(6):
+            pt = (2 * np.pi * nt + np.pi) / 4  # antiperiodic in t
+            px = 2 * np.pi * nx / 6
+            wr = 2.2 - np.cos(pt) - np.cos(px)
+            s = np.sqrt(np.sin(pt) ** 2 + np.sin(px) ** 2)
+            expect += [wr + 1j * s, wr - 1j * s]
+    def canon(v):
+        v = np.round(np.asarray(v), 9)
+        return v[np.lexsort((v.imag, v.real))]
+    assert np.allclose(canon(ev), canon(expect), atol=1e-8)

@@ -1,0 +1,13 @@
+"""B200 (sm_100a) implementation of the Wilson / domain-wall dynamical-fermion
+hot path of the 2-D U(1) lattice study, behind the C ABI in include/dwf_b200.h.
+
+The CUDA library (_lib/libdwfb200.so) is built by ``build.py``; without it every
+compute entry point raises.
+"""
+from . import _capi
+from ._capi import (OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD, SOLVER_CG64, SOLVER_MIXED, DwfError,
+                    LIB_PATH)
+from .dwf import DomainWall, CgResult
+
+__all__ = ["DomainWall", "CgResult", "DwfError", "OP_D", "OP_DDAG", "OP_DDDAG", "OP_DDAGD",
+           "SOLVER_CG64", "SOLVER_MIXED", "LIB_PATH"]

@@ -1,0 +1,88 @@
+"""ctypes binding of ``_lib/libdwfb200.so`` (the C ABI in include/dwf_b200.h).
+
+The library is required: importing a compute entry point without it raises,
+there is no CPU fallback.
+"""
+import ctypes as C
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "_lib" / "libdwfb200.so"
+
+DWF_OK, DWF_NOT_CONVERGED, DWF_ZERO_DENOM, DWF_NONFINITE = 0, 1, 2, 3
+DWF_CUDA_ERROR, DWF_TIMEOUT, DWF_BAD_ARG = 4, 5, 6
+OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD = 0, 1, 2, 3
+SOLVER_CG64, SOLVER_MIXED = 0, 1
+
+
+class DwfParams(C.Structure):
+    _fields_ = [("Nt", C.c_int), ("Nx", C.c_int), ("Ls", C.c_int),
+                ("M5", C.c_double), ("mf", C.c_double), ("beta", C.c_double),
+                ("device", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("status", C.c_int),
+                ("solver", C.c_int), ("relres", C.c_double), ("true_relres", C.c_double),
+                ("reliable_updates", C.c_int), ("fallback", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_DP = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "dwf_ctx_create": (_I, [C.POINTER(DwfParams), C.POINTER(_P)]),
+    "dwf_ctx_destroy": (_I, [_P]),
+    "dwf_status_string": (C.c_char_p, [_I]),
+    "dwf_last_error": (C.c_char_p, [_P]),
+    "dwf_set_wait_limit": (_I, [_P, C.c_uint64]),
+    "dwf_sync": (_I, [_P]),
+    "dwf_stream": (_P, [_P]),
+    "dwf_set_gauge": (_I, [_P, _I, _P]),
+    "dwf_set_gauge_dev": (_I, [_P, _I, _P]),
+    "dwf_apply": (_I, [_P, _I, _I, _P, _P, _I]),
+    "dwf_apply_dev": (_I, [_P, _I, _I, _P, _P, _I, _I]),
+    "dwf_cg": (_I, [_P, _I, _I, _P, _P, _I, _D, _I, _I, C.POINTER(SolveInfo)]),
+    "dwf_cg_batch_dev": (_I, [_P, _I, _I, _P, _P, _P, _I, _D, _I, _I, C.POINTER(SolveInfo)]),
+}
+
+_lib = None
+
+
+class DwfError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__(f"{status_string(status)}{': ' + msg if msg else ''}")
+
+
+def lib():
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with "
+                "`python -m three_part_dwf_study_b200.build` (no CPU fallback exists)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def status_string(status):
+    return lib().dwf_status_string(int(status)).decode()
+
+
+def check(status, ctx=None):
+    if status != DWF_OK:
+        msg = lib().dwf_last_error(ctx).decode() if ctx else ""
+        raise DwfError(status, msg)

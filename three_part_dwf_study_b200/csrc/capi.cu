@@ -1,0 +1,541 @@
+// C ABI: contexts, gauge upload, operator application and the batched solver.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "context.cuh"
+#include "kernels.cuh"
+
+using namespace dwfb;
+
+#define CK(call)                                                                        \
+    do                                                                                  \
+    {                                                                                   \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return ctx_fail(c, DWF_CUDA_ERROR, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace dwfb {
+
+int ctx_fail(dwf_ctx* c, int code, const std::string& msg)
+{
+    if (c)
+        c->err = msg;
+    return code;
+}
+
+namespace {
+
+template <typename T>
+int grow(dwf_ctx* c, T*& p, size_t n)
+{
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+    if (n == 0)
+        return DWF_OK;
+    CK(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)));
+    return DWF_OK;
+}
+
+}  // namespace
+
+int ensure_workspace(dwf_ctx* c, int nrhs)
+{
+    if (nrhs <= c->ws_rhs)
+        return DWF_OK;
+    CK(cudaStreamSynchronize(c->stream));
+    const size_t f = size_t(nrhs) * c->fsz();
+    int st;
+    if ((st = grow(c, c->w_r, f)) || (st = grow(c, c->w_p, f)) || (st = grow(c, c->w_t, f)) ||
+        (st = grow(c, c->w_b, f)) || (st = grow(c, c->w_x, f)) || (st = grow(c, c->w_r32, f)) ||
+        (st = grow(c, c->w_p32, f)) || (st = grow(c, c->w_t32, f)) ||
+        (st = grow(c, c->w_e32, f)) || (st = grow(c, c->w_conf, size_t(nrhs))) ||
+        (st = grow(c, c->w_active, size_t(nrhs))) || (st = grow(c, c->w_iters, size_t(nrhs))) ||
+        (st = grow(c, c->w_relres, size_t(nrhs))) || (st = grow(c, c->w_status, size_t(nrhs))) ||
+        (st = grow(c, c->w_ru, size_t(nrhs))) || (st = grow(c, c->w_true, size_t(nrhs))))
+    {
+        c->ws_rhs = 0;
+        return st;
+    }
+    c->ws_rhs = nrhs;
+    return DWF_OK;
+}
+
+int ensure_part(dwf_ctx* c, size_t n)
+{
+    if (n <= c->w_part_cap)
+        return DWF_OK;
+    CK(cudaStreamSynchronize(c->stream));
+    const int st = grow(c, c->w_part, n);
+    c->w_part_cap = st ? 0 : n;
+    return st;
+}
+
+int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const void* in,
+              void* out, int precision)
+{
+    if (nrhs < 1 || nrhs > 65535 || op < 0 || op > 3 || (precision != 64 && precision != 32))
+        return ctx_fail(c, DWF_BAD_ARG, "apply: bad op, nrhs or precision");
+    if (conf0 < 0 || conf0 >= c->nconf)
+        return ctx_fail(c, DWF_BAD_ARG, "apply: configuration index out of range (set_gauge first)");
+    const dim3 block(256);
+    const int bx = std::min((c->L.nsite + 255) / 256, std::max(1, 4 * c->nsm));
+    const dim3 grid(bx, nrhs);
+    const long fs = c->fsz();
+    const bool two = (op == DWF_OP_DDDAG || op == DWF_OP_DDAGD);
+    if (two)
+    {
+        const int st = ensure_workspace(c, nrhs);
+        if (st)
+            return st;
+    }
+    // first (or only) operator: D for D, D^dag D; D^dag for D^dag, D D^dag
+    const bool dag1 = (op == DWF_OP_DDAG || op == DWF_OP_DDDAG);
+    if (precision == 64)
+    {
+        const double2* src = static_cast<const double2*>(in);
+        double2* mid = two ? c->w_t : static_cast<double2*>(out);
+        if (dag1)
+            dirac_kernel<true, double><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U64, c->usz(), conf_d, conf0);
+        else
+            dirac_kernel<false, double><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U64, c->usz(), conf_d, conf0);
+        if (two)
+        {
+            if (dag1)
+                dirac_kernel<false, double><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<double2*>(out), fs, c->U64, c->usz(), conf_d, conf0);
+            else
+                dirac_kernel<true, double><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<double2*>(out), fs, c->U64, c->usz(), conf_d, conf0);
+        }
+    }
+    else
+    {
+        const float2* src = static_cast<const float2*>(in);
+        float2* mid = two ? c->w_t32 : static_cast<float2*>(out);
+        if (dag1)
+            dirac_kernel<true, float><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U32, c->usz(), conf_d, conf0);
+        else
+            dirac_kernel<false, float><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U32, c->usz(), conf_d, conf0);
+        if (two)
+        {
+            if (dag1)
+                dirac_kernel<false, float><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<float2*>(out), fs, c->U32, c->usz(), conf_d, conf0);
+            else
+                dirac_kernel<true, float><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<float2*>(out), fs, c->U32, c->usz(), conf_d, conf0);
+        }
+    }
+    CK(cudaGetLastError());
+    return DWF_OK;
+}
+
+int true_residual(dwf_ctx* c, int op, int nrhs, const int* conf_d, const double2* b,
+                  const double2* x, double* out)
+{
+    // t = D1 x
+    const bool dag1 = (op == DWF_OP_DDDAG);
+    const long fs = c->fsz();
+    const dim3 block(256);
+    const dim3 grid(std::min((c->L.nsite + 255) / 256, std::max(1, 4 * c->nsm)), nrhs);
+    if (dag1)
+        dirac_kernel<true, double><<<grid, block, 0, c->stream>>>(c->L, x, c->w_t, fs, c->U64, c->usz(), conf_d, 0);
+    else
+        dirac_kernel<false, double><<<grid, block, 0, c->stream>>>(c->L, x, c->w_t, fs, c->U64, c->usz(), conf_d, 0);
+    const int ch = 4096;
+    const int nch = (c->L.nsite + ch - 1) / ch;
+    int st = ensure_part(c, size_t(nrhs) * nch * 2);
+    if (st)
+        return st;
+    const dim3 g2(nch, nrhs);
+    if (dag1)
+        residual_partials_kernel<false><<<g2, block, 0, c->stream>>>(c->L, c->w_t, b, fs, c->U64, c->usz(), conf_d, nch, ch, c->w_part);
+    else
+        residual_partials_kernel<true><<<g2, block, 0, c->stream>>>(c->L, c->w_t, b, fs, c->U64, c->usz(), conf_d, nch, ch, c->w_part);
+    residual_finish_kernel<<<(nrhs + 7) / 8, 256, 0, c->stream>>>(c->w_part, nrhs, nch, c->w_true);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, c->w_true, nrhs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+namespace {
+
+constexpr int kSolverThreads = 256;
+constexpr int kMaxRhsPerLaunch = 2048;
+
+// One persistent launch over nrhs <= kMaxRhsPerLaunch right-hand sides.
+int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, double2* x,
+                  int has_guess, const int* active_d, double rtol, int maxiter, int eigen_rule,
+                  std::vector<int>& iters, std::vector<double>& relres, std::vector<int>& status,
+                  std::vector<int>& ru)
+{
+    SolveDesc d{};
+    d.L = c->L;
+    d.dag_first = (op == DWF_OP_DDDAG) ? 1 : 0;
+    d.nrhs = nrhs;
+    d.fsz = c->fsz();
+    d.rhs_conf = c->w_conf;
+    d.U64 = c->U64;
+    d.U32 = c->U32;
+    d.usz = c->usz();
+    d.b = b;
+    d.x = x;
+    d.r = c->w_r;
+    d.p = c->w_p;
+    d.t = c->w_t;
+    d.r32 = c->w_r32;
+    d.p32 = c->w_p32;
+    d.t32 = c->w_t32;
+    d.e32 = c->w_e32;
+    d.rtol = rtol;
+    d.maxiter = maxiter;
+    d.has_guess = has_guess;
+    d.active_in = active_d;
+    d.eigen_rule = eigen_rule;
+    d.delta = 0.1;
+    d.stall_limit = 3;
+    d.out_iters = c->w_iters;
+    d.out_relres = c->w_relres;
+    d.out_status = c->w_status;
+    d.out_ru = c->w_ru;
+    d.bar = c->bar;
+    d.timeout_ns = c->timeout_ns;
+
+    const void* fn = mixed ? reinterpret_cast<const void*>(&cg_mixed_kernel)
+                           : reinterpret_cast<const void*>(&cg64_kernel);
+    const size_t smem = solver_smem_bytes(nrhs);
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int bps = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kSolverThreads, smem));
+    if (bps < 1)
+        return ctx_fail(c, DWF_CUDA_ERROR, "solver kernel cannot be resident");
+    const int cap = bps * c->nsm;
+    // chunking: aim at about two units per block
+    const long total = long(nrhs) * c->L.nsite;
+    long ch = (total + 2L * cap - 1) / (2L * cap);
+    ch = ((ch + kSolverThreads - 1) / kSolverThreads) * kSolverThreads;
+    ch = std::max<long>(ch, kSolverThreads);
+    const long nsite_r = ((c->L.nsite + kSolverThreads - 1) / kSolverThreads) * kSolverThreads;
+    ch = std::min(ch, nsite_r);
+    d.ch = int(ch);
+    d.nch = int((c->L.nsite + ch - 1) / ch);
+    int st = ensure_part(c, size_t(nrhs) * d.nch * 2);
+    if (st)
+        return st;
+    d.part = c->w_part;
+    const int grid = int(std::min<long>(cap, long(nrhs) * d.nch));
+    d.expected_blocks = unsigned(grid);
+    CK(cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->stream));
+    void* args[] = {&d};
+    CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolverThreads), args, smem, c->stream));
+    GridBar hb{};
+    iters.resize(nrhs);
+    relres.resize(nrhs);
+    status.resize(nrhs);
+    ru.resize(nrhs);
+    CK(cudaMemcpyAsync(iters.data(), c->w_iters, nrhs * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(relres.data(), c->w_relres, nrhs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(status.data(), c->w_status, nrhs * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(ru.data(), c->w_ru, nrhs * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&hb, c->bar, sizeof(GridBar), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (hb.err != 0)
+        return ctx_fail(c, hb.err, hb.err == DWF_TIMEOUT ? "persistent solver: a grid barrier wait ran out"
+                                                          : "persistent solver: device error");
+    return DWF_OK;
+}
+
+}  // namespace
+
+int solve_batch(dwf_ctx* c, int op, int nrhs, const int* conf_h, const double2* b, double2* x,
+                int has_guess, double rtol, int maxiter, int solver, int eigen_rule,
+                dwf_solve_info* info)
+{
+    if (op != DWF_OP_DDDAG && op != DWF_OP_DDAGD)
+        return ctx_fail(c, DWF_BAD_ARG, "cg: op must be DWF_OP_DDDAG or DWF_OP_DDAGD");
+    if (nrhs < 1 || maxiter < 0 || !(rtol >= 0.0) || (solver != DWF_SOLVER_CG64 && solver != DWF_SOLVER_MIXED))
+        return ctx_fail(c, DWF_BAD_ARG, "cg: bad nrhs, maxiter, rtol or solver");
+    if (c->nconf < 1)
+        return ctx_fail(c, DWF_BAD_ARG, "cg: no gauge configuration (set_gauge first)");
+    for (int k = 0; conf_h && k < nrhs; ++k)
+        if (conf_h[k] < 0 || conf_h[k] >= c->nconf)
+            return ctx_fail(c, DWF_BAD_ARG, "cg: configuration index out of range");
+    const long fs = c->fsz();
+    for (int k0 = 0; k0 < nrhs; k0 += kMaxRhsPerLaunch)
+    {
+        const int n = std::min(kMaxRhsPerLaunch, nrhs - k0);
+        int st = ensure_workspace(c, n);
+        if (st)
+            return st;
+        std::vector<int> conf(n, 0);
+        if (conf_h)
+            std::copy(conf_h + k0, conf_h + k0 + n, conf.begin());
+        CK(cudaMemcpyAsync(c->w_conf, conf.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        const double2* bk = b + k0 * fs;
+        double2* xk = x + k0 * fs;
+        if (!has_guess)
+            CK(cudaMemsetAsync(xk, 0, size_t(n) * fs * sizeof(double2), c->stream));
+        std::vector<int> iters, status, ru;
+        std::vector<double> relres;
+        const bool mixed = (solver == DWF_SOLVER_MIXED);
+        st = launch_solver(c, mixed, op, n, bk, xk, has_guess, nullptr, rtol, maxiter, eigen_rule,
+                           iters, relres, status, ru);
+        if (st)
+            return st;
+        std::vector<int> fallback(n, 0);
+        int nfb = 0;
+        if (mixed)
+        {
+            for (int k = 0; k < n; ++k)
+                if (status[k] != DWF_OK)
+                {
+                    fallback[k] = 1;
+                    ++nfb;
+                }
+            if (nfb)
+            {
+                // plain FP64 CG from the mixed iterate for every right-hand side that stalled
+                CK(cudaMemcpyAsync(c->w_active, fallback.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+                std::vector<int> it2, st2, ru2;
+                std::vector<double> rr2;
+                st = launch_solver(c, false, op, n, bk, xk, 1, c->w_active, rtol, maxiter,
+                                   eigen_rule, it2, rr2, st2, ru2);
+                if (st)
+                    return st;
+                for (int k = 0; k < n; ++k)
+                    if (fallback[k])
+                    {
+                        iters[k] += it2[k];
+                        relres[k] = rr2[k];
+                        status[k] = st2[k];
+                    }
+            }
+        }
+        std::vector<double> tr(n);
+        st = true_residual(c, op, n, c->w_conf, bk, xk, tr.data());
+        if (st)
+            return st;
+        for (int k = 0; info && k < n; ++k)
+        {
+            dwf_solve_info& I = info[k0 + k];
+            I.iterations = iters[k];
+            I.status = status[k];
+            I.converged = status[k] == DWF_OK ? 1 : 0;
+            I.solver = solver;
+            I.relres = relres[k];
+            I.true_relres = tr[k];
+            I.reliable_updates = ru[k];
+            I.fallback = fallback[k];
+            if (!std::isfinite(tr[k]) && I.status == DWF_OK)
+                I.status = DWF_NONFINITE;
+        }
+    }
+    return DWF_OK;
+}
+
+}  // namespace dwfb
+
+// ---------------------------------------------------------------------------
+// exported entry points
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* dwf_status_string(int s)
+{
+    switch (s)
+    {
+    case DWF_OK: return "ok";
+    case DWF_NOT_CONVERGED: return "not converged";
+    case DWF_ZERO_DENOM: return "CG encountered a zero denominator";
+    case DWF_NONFINITE: return "non-finite value";
+    case DWF_CUDA_ERROR: return "CUDA error";
+    case DWF_TIMEOUT: return "device wait timed out";
+    case DWF_BAD_ARG: return "bad argument";
+    default: return "unknown status";
+    }
+}
+
+static int ctx_init(dwf_ctx* c, int device)
+{
+    c->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&c->bar, sizeof(GridBar)));
+    CK(cudaMemset(c->bar, 0, sizeof(GridBar)));
+    return DWF_OK;
+}
+
+int dwf_ctx_create(const dwf_params* p, dwf_ctx** out)
+{
+    if (!p || !out)
+        return DWF_BAD_ARG;
+    *out = nullptr;
+    if (p->Nt < 1 || p->Nx < 1 || p->Ls < 1 || long(p->Nt) * p->Nx * p->Ls > (1L << 30))
+        return DWF_BAD_ARG;
+    dwf_ctx* c = new dwf_ctx();
+    c->kind = 0;
+    c->L.Nt = p->Nt;
+    c->L.Nx = p->Nx;
+    c->L.Ls = p->Ls;
+    c->L.V = p->Nt * p->Nx;
+    c->L.nsite = p->Ls * c->L.V;
+    c->L.diag = 3.0 - p->M5;
+    c->L.mf = p->mf;
+    c->L.bct = -1.0;
+    c->L.bcx = 1.0;
+    c->L.fifth = 1;
+    c->beta = p->beta;
+    const int st = ctx_init(c, p->device);
+    if (st)
+    {
+        dwf_ctx_destroy(c);
+        return st;
+    }
+    *out = c;
+    return DWF_OK;
+}
+
+int dwf_ctx_destroy(dwf_ctx* c)
+{
+    if (!c)
+        return DWF_OK;
+    cudaSetDevice(c->device);
+    if (c->stream)
+        cudaStreamSynchronize(c->stream);
+    void* bufs[] = {c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_t, c->w_b, c->w_x,
+                    c->w_r32, c->w_p32, c->w_t32, c->w_e32, c->w_part, c->w_conf, c->w_active,
+                    c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar};
+    for (void* b : bufs)
+        if (b)
+            cudaFree(b);
+    if (c->stream)
+        cudaStreamDestroy(c->stream);
+    delete c;
+    return DWF_OK;
+}
+
+const char* dwf_last_error(const dwf_ctx* c) { return c ? c->err.c_str() : ""; }
+
+int dwf_set_wait_limit(dwf_ctx* c, uint64_t ns)
+{
+    if (!c || ns == 0)
+        return DWF_BAD_ARG;
+    c->timeout_ns = ns;
+    return DWF_OK;
+}
+
+int dwf_sync(dwf_ctx* c)
+{
+    if (!c)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+void* dwf_stream(dwf_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+static int set_gauge_impl(dwf_ctx* c, int nconf, const double* theta, cudaMemcpyKind kind)
+{
+    if (!c || nconf < 1 || !theta)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    const long n = long(nconf) * c->usz();
+    if (nconf > c->nconf_cap)
+    {
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->theta) cudaFree(c->theta);
+        if (c->U64) cudaFree(c->U64);
+        if (c->U32) cudaFree(c->U32);
+        c->theta = nullptr;
+        c->U64 = nullptr;
+        c->U32 = nullptr;
+        c->nconf_cap = 0;
+        CK(cudaMalloc(&c->theta, n * sizeof(double)));
+        CK(cudaMalloc(&c->U64, n * sizeof(double2)));
+        CK(cudaMalloc(&c->U32, n * sizeof(float2)));
+        c->nconf_cap = nconf;
+    }
+    CK(cudaMemcpyAsync(c->theta, theta, n * sizeof(double), kind, c->stream));
+    const int grid = int(std::min<long>((n + 255) / 256, 8L * c->nsm));
+    links_kernel<<<grid, 256, 0, c->stream>>>(c->theta, n, c->U64, c->U32);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    c->nconf = nconf;
+    return DWF_OK;
+}
+
+int dwf_set_gauge(dwf_ctx* c, int nconf, const double* theta)
+{
+    return set_gauge_impl(c, nconf, theta, cudaMemcpyHostToDevice);
+}
+
+int dwf_set_gauge_dev(dwf_ctx* c, int nconf, const double* theta_dev)
+{
+    return set_gauge_impl(c, nconf, theta_dev, cudaMemcpyDeviceToDevice);
+}
+
+int dwf_apply_dev(dwf_ctx* c, int op, int conf, const void* in, void* out, int nrhs, int precision)
+{
+    if (!c || !in || !out)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    return apply_dev(c, op, nrhs, nullptr, conf, in, out, precision);
+}
+
+int dwf_apply(dwf_ctx* c, int op, int conf, const double* in, double* out, int nrhs)
+{
+    if (!c || !in || !out || nrhs < 1)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    int st = ensure_workspace(c, nrhs);
+    if (st)
+        return st;
+    const size_t bytes = size_t(nrhs) * c->fsz() * sizeof(double2);
+    CK(cudaMemcpyAsync(c->w_b, in, bytes, cudaMemcpyHostToDevice, c->stream));
+    st = apply_dev(c, op, nrhs, nullptr, conf, c->w_b, c->w_x, 64);
+    if (st)
+        return st;
+    CK(cudaMemcpyAsync(out, c->w_x, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+int dwf_cg_batch_dev(dwf_ctx* c, int op, int nrhs, const int* rhs_conf, const void* b, void* x,
+                     int has_guess, double rtol, int maxiter, int solver, dwf_solve_info* info)
+{
+    if (!c || !b || !x)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    return solve_batch(c, op, nrhs, rhs_conf, static_cast<const double2*>(b),
+                       static_cast<double2*>(x), has_guess, rtol, maxiter, solver,
+                       c->kind == 1 ? 1 : 0, info);
+}
+
+int dwf_cg(dwf_ctx* c, int op, int conf, const double* b, double* x, int has_guess, double rtol,
+           int maxiter, int solver, dwf_solve_info* info)
+{
+    if (!c || !b || !x)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    // The staging buffers w_b / w_x must not be reallocated by the solver:
+    // size the workspace first.
+    int st = ensure_workspace(c, 1);
+    if (st)
+        return st;
+    const size_t bytes = c->fsz() * sizeof(double2);
+    CK(cudaMemcpyAsync(c->w_b, b, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (has_guess)
+        CK(cudaMemcpyAsync(c->w_x, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    st = solve_batch(c, op, 1, &conf, c->w_b, c->w_x, has_guess, rtol, maxiter, solver,
+                     c->kind == 1 ? 1 : 0, info);
+    if (st)
+        return st;
+    CK(cudaMemcpyAsync(x, c->w_x, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return info ? info->status : DWF_OK;
+}
+
+}  // extern "C"

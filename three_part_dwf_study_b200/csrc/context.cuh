@@ -1,0 +1,71 @@
+// Context: device, stream, gauge configurations and solver workspace.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "solver.cuh"
+
+struct dwf_ctx
+{
+    int kind = 0;  // 0 domain wall, 1 Wilson
+    dwfb::Lat L{};
+    double beta = 0.0;
+    int device = 0;
+    int nsm = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t timeout_ns = 5000000000ull;
+    std::string err;
+
+    // gauge configurations
+    int nconf = 0;
+    int nconf_cap = 0;
+    double* theta = nullptr;  // [nconf][2V]
+    double2* U64 = nullptr;
+    float2* U32 = nullptr;
+
+    // workspace, sized for ws_rhs right-hand sides
+    int ws_rhs = 0;
+    double2* w_r = nullptr;
+    double2* w_p = nullptr;
+    double2* w_t = nullptr;
+    double2* w_b = nullptr;  // host-pointer entry points stage b / in here
+    double2* w_x = nullptr;  // and x / out here
+    float2* w_r32 = nullptr;
+    float2* w_p32 = nullptr;
+    float2* w_t32 = nullptr;
+    float2* w_e32 = nullptr;
+    double* w_part = nullptr;
+    size_t w_part_cap = 0;
+    int* w_conf = nullptr;
+    int* w_active = nullptr;
+    int* w_iters = nullptr;
+    double* w_relres = nullptr;
+    int* w_status = nullptr;
+    int* w_ru = nullptr;
+    double* w_true = nullptr;
+    dwfb::GridBar* bar = nullptr;
+
+    long fsz() const { return 2L * L.nsite; }
+    long usz() const { return 2L * L.V; }
+};
+
+namespace dwfb {
+
+int ctx_fail(dwf_ctx* c, int code, const std::string& msg);
+int ensure_workspace(dwf_ctx* c, int nrhs);
+int ensure_part(dwf_ctx* c, size_t n);
+// Batched solve on device fields (b, x: nrhs fields of fsz complex doubles).
+int solve_batch(dwf_ctx* c, int op, int nrhs, const int* conf_h, const double2* b, double2* x,
+                int has_guess, double rtol, int maxiter, int solver, int eigen_rule,
+                dwf_solve_info* info);
+// FP64 true residual |b - A x| / |b| per right-hand side into host array out.
+int true_residual(dwf_ctx* c, int op, int nrhs, const int* conf_d, const double2* b,
+                  const double2* x, double* out);
+// out = op(in) on device fields, precision 64 or 32.
+int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const void* in,
+              void* out, int precision);
+
+}  // namespace dwfb

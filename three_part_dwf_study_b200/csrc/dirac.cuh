@@ -1,0 +1,148 @@
+// Wilson and domain-wall Dirac operators at one lattice site.
+//
+// Both operators share the 4-D hopping term
+//   (D psi)(y) = diag psi(y)
+//              - 1/2 sum_mu [ bc U_mu(y)       (1 - gamma_mu) psi(y + mu)
+//                           + bc U_mu(y - mu)^* (1 + gamma_mu) psi(y - mu) ]
+// with gamma_t = sigma1, gamma_x = sigma2 (domain_wall/include/spin.hpp:5-19,
+// wilson/include/wilson_operator.hpp:13-14). D^dag swaps (1 - gamma) and
+// (1 + gamma). diag = 3 - M5 for domain wall (dwf_operator.hpp:17), 2 + m0 for
+// Wilson (wilson_operator.hpp:35). Boundary signs: domain wall is
+// antiperiodic in t and periodic in x (dwf_operator.hpp:29-30); Wilson takes
+// them from wilson.time/space_boundary_sign (wilson_operator.hpp:38-54).
+//
+// Domain wall adds the fifth-dimension hop (dwf_operator.hpp:71-86 for D,
+// :150-165 for D^dag):
+//   D    : spin 1 gets -psi_1(s+1) (m_f psi_1(0) at s = Ls-1),
+//          spin 0 gets -psi_0(s-1) (m_f psi_0(Ls-1) at s = 0)
+//   D^dag: spin 1 gets -psi_1(s-1) (m_f psi_1(Ls-1) at s = 0),
+//          spin 0 gets -psi_0(s+1) (m_f psi_0(0) at s = Ls-1)
+//
+// Each hop is evaluated on its projected half-spinor: with
+// (1 + k gamma) v = (h, k g h) where h = v0 + k g^* v1 and g = 1 for
+// sigma1, g = i for sigma2, one complex link product per hop suffices.
+#pragma once
+
+#include "common.cuh"
+
+namespace dwfb {
+
+// Field loaders: dirac_site reads its input through one of these, so the
+// same stencil can read a stored field or a combination formed on the fly.
+template <typename R>
+struct FieldLd
+{
+    const cplx<R>* __restrict__ f;
+    __device__ __forceinline__ Spinor<R> sp(long site) const { return ld_spinor(f, site); }
+    __device__ __forceinline__ cplx<R> c(long idx) const { return f[idx]; }
+};
+
+// x + e with x in FP64 and e in FP32 (the mixed solver's reliable update).
+struct SumLd
+{
+    const double2* __restrict__ x;
+    const float2* __restrict__ e;
+    __device__ __forceinline__ Spinor<double> sp(long site) const
+    {
+        const Spinor<double> a = ld_spinor(x, site);
+        const Spinor<float> b = ld_spinor(e, site);
+        return {mkc(a.s0.x + double(b.s0.x), a.s0.y + double(b.s0.y)),
+                mkc(a.s1.x + double(b.s1.x), a.s1.y + double(b.s1.y))};
+    }
+    __device__ __forceinline__ double2 c(long idx) const
+    {
+        const double2 a = x[idx];
+        const float2 b = e[idx];
+        return mkc(a.x + double(b.x), a.y + double(b.y));
+    }
+};
+
+// Link phases are stored per configuration as U[mu][t][x] = (cos, sin).
+template <bool DAG, typename R, typename Ld>
+__device__ __forceinline__ Spinor<R> dirac_site_ld(const Ld& in, const cplx<R>* __restrict__ U,
+                                                const Lat& L, int s, int t, int x)
+{
+    using T = cplx<R>;
+    const int Nt = L.Nt, Nx = L.Nx;
+    const int tp = (t + 1 == Nt) ? 0 : t + 1;
+    const int tm = (t == 0) ? Nt - 1 : t - 1;
+    const int xp = (x + 1 == Nx) ? 0 : x + 1;
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+    const long sb = long(s) * L.V;
+    const int here = t * Nx + x;
+
+    const Spinor<R> c = in.sp(sb + here);
+    const Spinor<R> vtp = in.sp(sb + tp * Nx + x);
+    const Spinor<R> vtm = in.sp(sb + tm * Nx + x);
+    const Spinor<R> vxp = in.sp(sb + t * Nx + xp);
+    const Spinor<R> vxm = in.sp(sb + t * Nx + xm);
+    const T Ut = U[here];
+    const T Utm = U[tm * Nx + x];
+    const T Ux = U[L.V + here];
+    const T Uxm = U[L.V + t * Nx + xm];
+
+    const R stp = (t == Nt - 1) ? R(L.bct) : R(1);
+    const R stm = (t == 0) ? R(L.bct) : R(1);
+    const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
+    const R sxm = (x == 0) ? R(L.bcx) : R(1);
+    // forward hops use (1 + kf gamma), backward hops (1 + kb gamma)
+    constexpr R kf = DAG ? R(1) : R(-1);
+    constexpr R kb = -kf;
+
+    T w = cmul(Ut, stp * (vtp.s0 + kf * vtp.s1));
+    T up = w;
+    T lo = kf * w;
+    w = cmulc(Utm, stm * (vtm.s0 + kb * vtm.s1));
+    up += w;
+    lo += kb * w;
+    w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
+    up += w;
+    lo += kf * itimes(w);
+    w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
+    up += w;
+    lo += kb * itimes(w);
+
+    const R dg = R(L.diag);
+    Spinor<R> o;
+    o.s0 = dg * c.s0 - R(0.5) * up;
+    o.s1 = dg * c.s1 - R(0.5) * lo;
+
+    if (L.fifth)
+    {
+        const int Ls = L.Ls;
+        const int sup = (s + 1 == Ls) ? 0 : s + 1;
+        const R cup = (s + 1 == Ls) ? R(L.mf) : R(-1);
+        const int sdn = (s == 0) ? Ls - 1 : s - 1;
+        const R cdn = (s == 0) ? R(L.mf) : R(-1);
+        if (!DAG)
+        {
+            o.s1 += cup * in.c(2 * (long(sup) * L.V + here) + 1);
+            o.s0 += cdn * in.c(2 * (long(sdn) * L.V + here));
+        }
+        else
+        {
+            o.s1 += cdn * in.c(2 * (long(sdn) * L.V + here) + 1);
+            o.s0 += cup * in.c(2 * (long(sup) * L.V + here));
+        }
+    }
+    return o;
+}
+
+template <bool DAG, typename R>
+__device__ __forceinline__ Spinor<R> dirac_site(const cplx<R>* __restrict__ in,
+                                                const cplx<R>* __restrict__ U, const Lat& L,
+                                                int s, int t, int x)
+{
+    return dirac_site_ld<DAG, R>(FieldLd<R>{in}, U, L, s, t, x);
+}
+
+// Site index i in [0, Ls*V) -> (s, t, x), x fastest (the reference layout).
+__device__ __forceinline__ void site_coords(const Lat& L, int i, int& s, int& t, int& x)
+{
+    s = i / L.V;
+    const int r = i - s * L.V;
+    t = r / L.Nx;
+    x = r - t * L.Nx;
+}
+
+}  // namespace dwfb

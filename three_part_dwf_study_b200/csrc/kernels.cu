@@ -1,0 +1,105 @@
+// Non-persistent kernels: link phases, standalone operator application and
+// the FP64 true residual.
+#include "kernels.cuh"
+
+namespace dwfb {
+
+__global__ void links_kernel(const double* __restrict__ theta, long n, double2* __restrict__ U64,
+                             float2* __restrict__ U32)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n;
+         i += long(gridDim.x) * blockDim.x)
+    {
+        double sn, cs;
+        sincos(theta[i], &sn, &cs);
+        U64[i] = make_double2(cs, sn);
+        U32[i] = make_float2(float(cs), float(sn));
+    }
+}
+
+template <bool DAG, typename R>
+__global__ void __launch_bounds__(256)
+    dirac_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out, long fsz,
+                 const cplx<R>* __restrict__ U, long usz, const int* __restrict__ conf,
+                 int conf0)
+{
+    const int j = blockIdx.y;
+    const int c = conf ? conf[j] : conf0;
+    const cplx<R>* Uj = U + long(c) * usz;
+    const cplx<R>* inj = in + j * fsz;
+    cplx<R>* outj = out + j * fsz;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.nsite; i += gridDim.x * blockDim.x)
+    {
+        int s, t, x;
+        site_coords(L, i, s, t, x);
+        st_spinor(outj, i, dirac_site<DAG, R>(inj, Uj, L, s, t, x));
+    }
+}
+
+template __global__ void dirac_kernel<false, double>(Lat, const double2*, double2*, long,
+                                                     const double2*, long, const int*, int);
+template __global__ void dirac_kernel<true, double>(Lat, const double2*, double2*, long,
+                                                    const double2*, long, const int*, int);
+template __global__ void dirac_kernel<false, float>(Lat, const float2*, float2*, long,
+                                                    const float2*, long, const int*, int);
+template __global__ void dirac_kernel<true, float>(Lat, const float2*, float2*, long,
+                                                   const float2*, long, const int*, int);
+
+template <bool DAG>
+__global__ void __launch_bounds__(256)
+    residual_partials_kernel(Lat L, const double2* __restrict__ t, const double2* __restrict__ b,
+                             long fsz, const double2* __restrict__ U, long usz,
+                             const int* __restrict__ conf, int nch, int ch,
+                             double* __restrict__ part)
+{
+    __shared__ double scratch[64];
+    const int j = blockIdx.y, c = blockIdx.x;
+    const double2* Uj = U + long(conf[j]) * usz;
+    const int beg = c * ch, end = min(beg + ch, L.nsite);
+    double rr = 0.0, bb = 0.0;
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x)
+    {
+        int s, tt, x;
+        site_coords(L, i, s, tt, x);
+        const Spinor<double> a = dirac_site<DAG, double>(t + j * fsz, Uj, L, s, tt, x);
+        const Spinor<double> bv = ld_spinor(b + j * fsz, i);
+        const Spinor<double> r = {bv.s0 - a.s0, bv.s1 - a.s1};
+        rr += spinor_norm2(r);
+        bb += spinor_norm2(bv);
+    }
+    rr = block_sum(rr, scratch);
+    bb = block_sum(bb, scratch);
+    if (threadIdx.x == 0)
+    {
+        part[(long(j) * nch + c) * 2] = rr;
+        part[(long(j) * nch + c) * 2 + 1] = bb;
+    }
+}
+
+template __global__ void residual_partials_kernel<false>(Lat, const double2*, const double2*,
+                                                         long, const double2*, long, const int*,
+                                                         int, int, double*);
+template __global__ void residual_partials_kernel<true>(Lat, const double2*, const double2*, long,
+                                                        const double2*, long, const int*, int,
+                                                        int, double*);
+
+__global__ void residual_finish_kernel(const double* __restrict__ part, int nrhs, int nch,
+                                       double* __restrict__ out)
+{
+    const int lane = threadIdx.x & 31;
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (j >= nrhs)
+        return;
+    double rr = 0.0, bb = 0.0;
+    for (int c = lane; c < nch; c += 32)
+    {
+        rr += part[(long(j) * nch + c) * 2];
+        bb += part[(long(j) * nch + c) * 2 + 1];
+    }
+    rr = warp_sum(rr);
+    bb = warp_sum(bb);
+    if (lane == 0)
+        out[j] = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+}
+
+}  // namespace dwfb

@@ -1,0 +1,31 @@
+// Non-persistent kernels: link phases, operator application, residual norms.
+#pragma once
+
+#include "dirac.cuh"
+
+namespace dwfb {
+
+// theta[c][mu][t][x] -> U64 = (cos, sin), U32 = rounded copy.
+__global__ void links_kernel(const double* __restrict__ theta, long n, double2* __restrict__ U64,
+                             float2* __restrict__ U32);
+
+// out[j] = D or D^dag (in[j]) on configuration conf[j] (conf may be null -> conf0).
+template <bool DAG, typename R>
+__global__ void dirac_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                             long fsz, const cplx<R>* __restrict__ U, long usz,
+                             const int* __restrict__ conf, int conf0);
+
+// Per-(rhs, chunk) partials of |b - D2 t|^2 and |b|^2 (true residual of A x = b
+// after t = D1 x).
+template <bool DAG>
+__global__ void residual_partials_kernel(Lat L, const double2* __restrict__ t,
+                                         const double2* __restrict__ b, long fsz,
+                                         const double2* __restrict__ U, long usz,
+                                         const int* __restrict__ conf, int nch, int ch,
+                                         double* __restrict__ part);
+
+// out[j] = sqrt(sum part[j][.][0] / sum part[j][.][1]), one warp per rhs.
+__global__ void residual_finish_kernel(const double* __restrict__ part, int nrhs, int nch,
+                                       double* __restrict__ out);
+
+}  // namespace dwfb

@@ -1,0 +1,61 @@
+// Persistent multi-right-hand-side CG kernels.
+#pragma once
+
+#include "dirac.cuh"
+
+namespace dwfb {
+
+// Per-right-hand-side state codes held in shared memory during a solve.
+enum : int
+{
+    RHS_ACTIVE = -1,
+};
+
+struct SolveDesc
+{
+    Lat L;
+    int dag_first;  // 1: A = D D^dag (D^dag applied first); 0: A = D^dag D
+    int nrhs;
+    long fsz;       // complex elements per right-hand-side field (2 * nsite)
+    const int* rhs_conf;  // device [nrhs] configuration index per right-hand side
+    const double2* U64;   // [nconf][2V]
+    const float2* U32;
+    long usz;             // link elements per configuration (2V)
+    const double2* b;
+    double2* x;
+    double2* r;
+    double2* p;
+    double2* t;
+    float2* r32;
+    float2* p32;
+    float2* t32;
+    float2* e32;
+    double* part;  // partial sums [nrhs][nch][2]
+    int nch, ch;   // chunks per right-hand side and sites per chunk
+    double rtol;
+    int maxiter;
+    int has_guess;
+    const int* active_in;  // device [nrhs] or null: right-hand sides with 0 are left untouched
+    int eigen_rule;   // stop at |r|^2 < tol^2 |b|^2 and count as Eigen's ConjugateGradient
+    double delta;     // reliable-update trigger: |r32| < delta * |r| at the last update
+    int stall_limit;  // consecutive non-improving reliable updates before giving up
+    // outputs (device, [nrhs])
+    int* out_iters;
+    double* out_relres;
+    int* out_status;
+    int* out_ru;
+    GridBar* bar;
+    unsigned long long timeout_ns;
+    unsigned expected_blocks;  // normally gridDim.x
+};
+
+// Dynamic shared memory needed by the solver kernels for nrhs right-hand sides.
+inline size_t solver_smem_bytes(int nrhs)
+{
+    return 64 * sizeof(double) + size_t(nrhs) * (5 * sizeof(double) + 5 * sizeof(int));
+}
+
+__global__ void cg64_kernel(SolveDesc d);
+__global__ void cg_mixed_kernel(SolveDesc d);
+
+}  // namespace dwfb

@@ -1,0 +1,191 @@
+"""Host-side mirror of the reference's domain-wall entry points over the C ABI.
+
+Names, argument meaning and error behaviour follow the reference headers:
+    apply_D, apply_D_dagger, apply_DD_dagger, apply_D_dagger_D
+        (domain_wall/include/dwf_operator.hpp:15-181)
+    conjugate_gradient -> CgResult(x, iterations, relative_residual, converged)
+        (domain_wall/include/cg_solver.hpp:9-64; raises "CG encountered a zero
+         denominator" where the reference throws, :45-46)
+Fields are numpy complex128 arrays in the reference layout
+((s*Nt + t)*Nx + x)*2 + spin; theta is float64 (mu*Nt + t)*Nx + x.
+Device entry points (suffix _dev) take torch CUDA tensors.
+"""
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi as A
+
+
+@dataclass
+class CgResult:
+    x: np.ndarray
+    iterations: int
+    relative_residual: float
+    converged: bool
+    info: dict = field(default_factory=dict)
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class DomainWall:
+    """One device context for a domain-wall lattice (dwf.Nt, dwf.Nx, dwf.N5,
+    dwf.M5, dwf.mf, dwf.beta)."""
+
+    def __init__(self, Nt, Nx, Ls, M5, mf, beta=0.0, device=0):
+        self.Nt, self.Nx, self.Ls = int(Nt), int(Nx), int(Ls)
+        self.M5, self.mf, self.beta = float(M5), float(mf), float(beta)
+        self.device = int(device)
+        self.Ndof = self.Ls * self.Nt * self.Nx * 2
+        self.Ngauge = 2 * self.Nt * self.Nx
+        p = A.DwfParams(self.Nt, self.Nx, self.Ls, self.M5, self.mf, self.beta, self.device)
+        h = C.c_void_p()
+        A.check(A.lib().dwf_ctx_create(C.byref(p), C.byref(h)))
+        self._h = h
+        self._theta = None
+
+    @classmethod
+    def from_parameters(cls, p, device=0):
+        return cls(p["Nt"], p["Nx"], p["N5"], p["M5"], p["mf"], p["beta"], device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            A.lib().dwf_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, st):
+        A.check(st, self._h)
+
+    # ---- gauge ---------------------------------------------------------------
+    def set_gauge(self, thetas):
+        th = np.ascontiguousarray(thetas, dtype=np.float64)
+        n = th.size // self.Ngauge
+        if n * self.Ngauge != th.size or n < 1:
+            raise ValueError("theta size is not a multiple of 2*Nt*Nx")
+        self._check(A.lib().dwf_set_gauge(self._h, n, _ptr(th)))
+        self._theta = th.reshape(n, self.Ngauge).copy() if n == 1 else None
+
+    def _ensure(self, theta):
+        th = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+        if th.size != self.Ngauge:
+            raise ValueError("theta must hold 2*Nt*Nx link angles")
+        if self._theta is None or not np.array_equal(self._theta[0], th):
+            self.set_gauge(th)
+
+    # ---- operators (reference names) ------------------------------------------
+    def apply(self, op, theta, psi):
+        self._ensure(theta)
+        v = np.ascontiguousarray(psi, dtype=np.complex128)
+        nrhs = v.size // self.Ndof
+        if nrhs * self.Ndof != v.size:
+            raise ValueError("field size is not a multiple of Ndof")
+        out = np.empty_like(v)
+        self._check(A.lib().dwf_apply(self._h, op, 0, _ptr(v), _ptr(out), nrhs))
+        return out
+
+    def apply_D(self, theta, psi):
+        return self.apply(A.OP_D, theta, psi)
+
+    def apply_D_dagger(self, theta, psi):
+        return self.apply(A.OP_DDAG, theta, psi)
+
+    def apply_DD_dagger(self, theta, psi):
+        return self.apply(A.OP_DDDAG, theta, psi)
+
+    def apply_D_dagger_D(self, theta, psi):
+        return self.apply(A.OP_DDAGD, theta, psi)
+
+    def conjugate_gradient(self, op, theta, b, initial_guess=None, rtol=1e-10, maxiter=1000,
+                           solver=A.SOLVER_CG64):
+        """CG on op in {OP_DDDAG, OP_DDAGD}; mirrors cg_solver.hpp:17-64."""
+        self._ensure(theta)
+        bb = np.ascontiguousarray(b, dtype=np.complex128)
+        if bb.size != self.Ndof:
+            raise ValueError("b must hold Ndof complex entries")
+        if initial_guess is not None:
+            x = np.array(initial_guess, dtype=np.complex128, copy=True).reshape(-1)
+        else:
+            x = np.zeros(self.Ndof, np.complex128)
+        info = A.SolveInfo()
+        st = A.lib().dwf_cg(self._h, op, 0, _ptr(bb), _ptr(x), int(initial_guess is not None),
+                            float(rtol), int(maxiter), int(solver), C.byref(info))
+        if st == A.DWF_ZERO_DENOM:
+            raise RuntimeError("CG encountered a zero denominator")
+        if st not in (A.DWF_OK, A.DWF_NOT_CONVERGED):
+            self._check(st)
+        return CgResult(x, info.iterations, info.relres, bool(info.converged), info.as_dict())
+
+    # ---- device entry points (torch tensors) -----------------------------------------
+    def _dev_fields(self, t, what):
+        """(precision, nrhs) of a contiguous CUDA tensor holding whole fields.
+        float64/complex128 -> FP64, float32/complex64 -> FP32; the byte count
+        must be an exact multiple of one field."""
+        import torch
+        if not t.is_cuda or not t.is_contiguous():
+            raise ValueError(f"{what}: expected a contiguous CUDA tensor")
+        if t.dtype in (torch.float64, torch.complex128):
+            prec, csize = 64, 16
+        elif t.dtype in (torch.float32, torch.complex64):
+            prec, csize = 32, 8
+        else:
+            raise ValueError(f"{what}: unsupported dtype {t.dtype}")
+        nbytes = t.numel() * t.element_size()
+        per = self.Ndof * csize
+        if nbytes == 0 or nbytes % per:
+            raise ValueError(f"{what}: {nbytes} bytes is not a whole number of fields")
+        return prec, nbytes // per
+
+    def set_gauge_dev(self, thetas):
+        import torch
+        if not thetas.is_cuda or thetas.dtype != torch.float64 or not thetas.is_contiguous():
+            raise ValueError("thetas: expected a contiguous CUDA float64 tensor")
+        n = thetas.numel() // self.Ngauge
+        if n < 1 or n * self.Ngauge != thetas.numel():
+            raise ValueError("thetas: size is not a multiple of 2*Nt*Nx")
+        self._check(A.lib().dwf_set_gauge_dev(self._h, n, C.c_void_p(thetas.data_ptr())))
+        self._theta = None
+
+    def apply_dev(self, op, inp, out, conf=0):
+        prec, nrhs = self._dev_fields(inp, "in")
+        prec2, nrhs2 = self._dev_fields(out, "out")
+        if (prec, nrhs) != (prec2, nrhs2):
+            raise ValueError("in/out: precision or field count differ")
+        self._check(A.lib().dwf_apply_dev(self._h, op, conf, C.c_void_p(inp.data_ptr()),
+                                          C.c_void_p(out.data_ptr()), nrhs, prec))
+
+    def cg_batch_dev(self, op, b, x, rhs_conf=None, has_guess=False, rtol=1e-10, maxiter=1000,
+                     solver=A.SOLVER_CG64):
+        prec, nrhs = self._dev_fields(b, "b")
+        prec2, nrhs2 = self._dev_fields(x, "x")
+        if prec != 64 or prec2 != 64 or nrhs2 != nrhs:
+            raise ValueError("b/x: expected FP64 fields of equal count")
+        infos = (A.SolveInfo * nrhs)()
+        conf = None
+        if rhs_conf is not None:
+            conf = np.ascontiguousarray(rhs_conf, dtype=np.int32).reshape(-1)
+            if conf.size != nrhs:
+                raise ValueError(f"rhs_conf: {conf.size} entries for {nrhs} right-hand sides")
+        self._check(A.lib().dwf_cg_batch_dev(
+            self._h, op, nrhs, _ptr(conf) if conf is not None else None,
+            C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), int(has_guess), float(rtol),
+            int(maxiter), int(solver), infos))
+        return [i.as_dict() for i in infos]
+
+    def sync(self):
+        self._check(A.lib().dwf_sync(self._h))
+
+    def stream_ptr(self):
+        return A.lib().dwf_stream(self._h)

@@ -1,0 +1,551 @@
+#!/usr/bin/env python3
+"""Benchmark: domain-wall propagator solves per second to a true FP64
+residual of 1e-10 on one B200, and the standalone Dslash bandwidth.
+
+Workload (one "step"): the per-configuration propagator set of the
+domain-wall analyzer on a 64x64 lattice, Ls = 16, M5 = 1.0, m_f = 0.05 with a
+seeded hot-start gauge field (theta uniform in [-pi, pi)): 2 spins x 4 source
+times boundary point sources, 16 complex Z4 boundary-noise sources and
+2 spins x 2 source times boundary wall sources (28 right-hand sides), each
+solved as x = (D^dag D)^-1 D^dag src (domain_wall/include/correlator.hpp
+:60-79, :129-142, :197-220) until the FP64 true residual of the normal
+equation is <= 1e-10.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0. `value` = right-hand sides solved per second across
+all ranks, inputs resident in HBM, CUDA-event device time, max over ranks;
+`e2e` = the same through the host C-ABI entry (dwf_set_gauge + dwf_propagators
+from pinned host buffers, solutions read back). With --gpus N (torchrun) every
+rank solves its own configuration's set (weak scaling, no exchange).
+`--impl reference` times the reference's own CPU solver (oracle/_ref/ref_bench,
+the reference's conjugate_gradient + apply_D_dagger_D compiled from its
+sources) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+NT, NX, LS = 64, 64, 16
+M5, MF, BETA = 1.0, 0.05, 3.0
+RTOL = 1.0e-10
+MAXITER = 20000
+POINT_TIMES = (0, 16, 32, 48)
+WALL_TIMES = (0, 32)
+N_NOISE = 16
+GAUGE_SEED = 20260101
+NOISE_SEED = 918273
+REF_ITERS_FILE = REPO / "oracle" / "bench_ref_iters.json"
+REF_BENCH = REPO / "oracle" / "_ref" / "ref_bench"
+DSLASH_LATTICE = (512, 512, 16)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_gauge(rank):
+    rng = np.random.default_rng(GAUGE_SEED + 7919 * rank)
+    return rng.uniform(-np.pi, np.pi, 2 * NT * NX)
+
+
+def fi(s, t, x, a):
+    return ((s * NT + t) * NX + x) * 2 + a
+
+
+def workload_sources(rank):
+    """28 boundary sources (complex128 [28, Ndof]). P_L = diag(0, 1),
+    P_R = diag(1, 0): spin 1 of the source sits on s = 0, spin 0 on s = Ls-1
+    (correlator.hpp:133-138, :201-211, :60-75)."""
+    ndof = LS * NT * NX * 2
+    srcs = []
+    for t in POINT_TIMES:
+        for b in (0, 1):
+            v = np.zeros(ndof, np.complex128)
+            if b == 1:
+                v[fi(0, t, 0, 1)] = 1.0
+            else:
+                v[fi(LS - 1, t, 0, 0)] = 1.0
+            srcs.append(v)
+    rng = np.random.default_rng(NOISE_SEED + 104729 * rank)
+    phases = np.array([1, 1j, -1, -1j])
+    for _ in range(N_NOISE):
+        eta = phases[rng.integers(0, 4, size=(NT, NX, 2))]
+        v = np.zeros((LS, NT, NX, 2), np.complex128)
+        v[0, :, :, 1] = eta[:, :, 1]
+        v[LS - 1, :, :, 0] += eta[:, :, 0]
+        srcs.append(v.ravel())
+    for t in WALL_TIMES:
+        for b in (0, 1):
+            v = np.zeros((LS, NT, NX, 2), np.complex128)
+            if b == 1:
+                v[0, t, :, 1] = 1.0
+            else:
+                v[LS - 1, t, :, 0] = 1.0
+            srcs.append(v.ravel())
+    return np.stack(srcs)
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes (per right-hand side)
+# ---------------------------------------------------------------------------
+def dslash_bytes(V, Ls, w):
+    """One D or D^dag application: every spinor read once and written once,
+    links (complex) shared by the Ls slices: V * (Ls * 2 * 4w + 2 * 2w)."""
+    return V * (Ls * 2 * 4 * w + 2 * 2 * w)
+
+
+def cg_iter_bytes(V, Ls, w):
+    """One CG iteration on D^dag D: two Dslash plus ten spinor streams."""
+    return 2 * dslash_bytes(V, Ls, w) + 10 * V * Ls * 4 * w
+
+
+def reliable_update_bytes(V, Ls):
+    """FP64 residual replacement: two FP64 Dslash plus x, e, b reads and
+    x, r, r32, e writes."""
+    return 2 * dslash_bytes(V, Ls, 8) + V * Ls * (32 + 16 + 32 + 32 + 32 + 16 + 16)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        smax = max(r[1] for r in rows)
+        loaded = [r for r in rows if r[0] > 0.5 * smax] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[2]) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": smax,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (the reference's own solver, compiled from its sources)
+# ---------------------------------------------------------------------------
+def ref_params_text(maxiter):
+    keys = {
+        "wilson.Nt": 8, "wilson.Nx": 8, "wilson.beta": 2.0, "wilson.m0": 0.1,
+        "wilson.trajectories": 1, "wilson.thermalization_cut": 0, "wilson.thin": 1,
+        "wilson.hmc_steps": 1, "wilson.trajectory_length": 1.0, "wilson.source_t": 0,
+        "wilson.source_x": 0, "wilson.time_boundary_sign": -1.0,
+        "wilson.space_boundary_sign": 1.0, "wilson.force_cg_tolerance": 1e-10,
+        "wilson.force_cg_max_iterations": 1, "wilson.measurement_cg_tolerance": 1e-10,
+        "wilson.measurement_cg_max_iterations": 1, "wilson.random_seed": 1,
+        "dwf.Nt": NT, "dwf.Nx": NX, "dwf.N5": LS, "dwf.beta": BETA, "dwf.M5": M5,
+        "dwf.mf": MF, "dwf.epsilon": 0.01, "dwf.leapfrog_steps": 1, "dwf.trajectories": 1,
+        "dwf.thermalization_cut": 0, "dwf.thin": 1, "dwf.pseudofermion_rtol": RTOL,
+        "dwf.pseudofermion_maxiter": maxiter, "dwf.propagator_rtol": RTOL,
+        "dwf.propagator_maxiter": maxiter, "dwf.random_seed": 1, "eta.noise_vectors": 1,
+        "eta.random_seed": 1, "eta.flavors": 2, "analysis.threads": 0,
+        "analysis.plateau_window_size": 2, "analysis.plateau_flatness_tolerance": 0.1,
+        "analysis.earliest_plateau_time": 1, "analysis.fit_t_min": 1, "analysis.fit_t_max": 2,
+        "analysis.gevp_t0": 1, "analysis.max_momentum": 1, "analysis.bootstrap_resamples": 1,
+        "analysis.bootstrap_block_size": 1, "analysis.bootstrap_seed": 1,
+    }
+    return "".join(f"{k} = {v!r}\n" if isinstance(v, float) else f"{k} = {v}\n"
+                   for k, v in keys.items())
+
+
+def run_ref_bench(nsolves, threads, maxiter, rank=0):
+    """Run the reference's solver on `nsolves` point sources, capped at
+    `maxiter` CG iterations each; returns the driver's JSON."""
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        (d / "parameters.txt").write_text(ref_params_text(maxiter))
+        np.save(d / "in_theta.npy", workload_gauge(rank).reshape(2, NT, NX))
+        r = subprocess.run([str(REF_BENCH), str(nsolves), str(threads)], cwd=d,
+                           capture_output=True, text=True, timeout=1800)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_bench failed: {r.stderr.strip()}")
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def reference_full_iterations():
+    """Iterations the reference's CG needs for each of the 8 point sources of
+    the rank-0 workload (calibrated once by --calibrate-reference)."""
+    if REF_ITERS_FILE.exists():
+        return json.loads(REF_ITERS_FILE.read_text())["iterations"]
+    return None
+
+
+def cpu_sample(threads, budget_s=15.0):
+    """Bounded sample of the reference on `threads` host threads: `threads`
+    point-source solves run concurrently, each capped at a number of CG
+    iterations sized to about budget_s, scaled to full solves with the
+    calibrated iteration counts. Returns (solves/s, description, kind)."""
+    full = reference_full_iterations()
+    if not REF_BENCH.exists() or full is None:
+        return None
+    probe = run_ref_bench(threads, threads, 10)
+    per_iter = probe["seconds"] / 10.0
+    cap = int(max(20, min(min(full), budget_s / max(per_iter, 1e-6))))
+    res = run_ref_bench(threads, threads, cap)
+    done = [min(i, cap) for i in res["iterations"]]
+    need = [full[i % 8] for i in range(threads)]
+    # each thread runs one solve; a full solve needs need/done times the sample
+    est_full_seconds = res["seconds"] * max(n / max(d, 1) for n, d in zip(need, done))
+    sps = threads / est_full_seconds
+    desc = (f"{threads} concurrent point-source solves (one per thread), each capped at "
+            f"{cap} CG iterations ({res['seconds']:.2f} s), scaled to full solves of "
+            f"{min(need)}-{max(need)} iterations (reference iteration counts to rtol "
+            f"{RTOL:g}, calibrated from full runs of the same solver)")
+    return sps, desc, res["seconds"]
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def impl_reference(args):
+    ws, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    full = reference_full_iterations()
+    if not REF_BENCH.exists() or full is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_bench or its iteration calibration "
+                                         "is missing"}))
+        return 0
+    per_step = []
+    budget = max(5.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    desc = ""
+    for k in range(args.warmup + args.steps):
+        sps, desc, secs = cpu_sample(threads, budget)
+        if k >= args.warmup:
+            per_step.append(sps)
+    value = statistics.mean(per_step)
+    line = {
+        "impl": "reference", "metric": "dwf_propagator_solves_per_s_true_res_1e-10",
+        "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 28 / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config("reference CPU CG (FP64)"),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads,
+                         "kind": "reference", "sample": desc},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(solver):
+    return {
+        "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, seeded hot "
+                     f"start, 28 boundary sources per step (8 point, 16 Z4 noise, 4 wall), "
+                     f"to FP64 true residual {RTOL:g} of D^dag D"),
+        "lattice": [NT, NX, LS], "rhs_per_step": 28, "rtol": RTOL, "solver": solver,
+        "l2": "flushed between steps (256 MiB write)",
+    }
+
+
+def impl_ours(args):
+    import torch
+    ws, rank, local = dist_setup()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    import three_part_dwf_study_b200 as T
+
+    dev = torch.device("cuda", local)
+    d = T.DomainWall(NT, NX, LS, M5, MF, BETA, device=local)
+    theta = workload_gauge(rank)
+    d.set_gauge(theta)
+    srcs = workload_sources(rank)
+    nrhs = srcs.shape[0]
+    src_dev = torch.from_numpy(srcs.view(np.float64).copy()).to(dev)
+    x_dev = torch.zeros_like(src_dev)
+    stream = torch.cuda.ExternalStream(d.stream_ptr(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(fn, steps, warmup, tag):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        total = 0.0
+        k0, n0 = d.solver_kernel_ms()
+        l0 = d.launch_count()
+        infos_all = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            infos_all.append(fn())
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1) * 1e-3
+        barrier()
+        k1, n1 = d.solver_kernel_ms()
+        return total, infos_all, (k1 - k0) * 1e-3, n1 - n0, d.launch_count() - l0
+
+    def step_mixed():
+        return d.propagators_dev(src_dev, x_dev, rtol=RTOL, maxiter=MAXITER,
+                                 solver=T.SOLVER_MIXED)
+
+    def step_fp64():
+        return d.propagators_dev(src_dev, x_dev, rtol=RTOL, maxiter=MAXITER,
+                                 solver=T.SOLVER_CG64)
+
+    with ClockSampler(local) as clk:
+        t_mixed, infos_m, kern_s, nkern, launches = timed(step_mixed, args.steps, args.warmup,
+                                                          "mixed")
+    clocks = clk.summary()
+    t_fp64, infos_f, kern64_s, nkern64, _ = timed(step_fp64, max(1, args.steps // 2), 1, "fp64")
+
+    for infos in infos_m + infos_f:
+        for i in infos:
+            if not i["converged"] or i["true_relres"] > RTOL * 1.0001:
+                raise SystemExit(f"solve did not reach the FP64 true residual: {i}")
+
+    # max over ranks of device time
+    def allmax(v):
+        if ws == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t_mixed_max = allmax(t_mixed)
+    t_fp64_max = allmax(t_fp64)
+    value = ws * nrhs * args.steps / t_mixed_max
+    fp64_value = ws * nrhs * max(1, args.steps // 2) / t_fp64_max
+
+    # ---- end to end through the host C ABI ----
+    src_host = torch.from_numpy(srcs.view(np.float64).copy()).pin_memory()
+    x_host = torch.empty_like(src_host).pin_memory()
+    th_host = torch.from_numpy(theta.copy()).pin_memory()
+    src_np = src_host.numpy().view(np.complex128)
+    x_np = x_host.numpy().view(np.complex128)
+    th_np = th_host.numpy()
+
+    import ctypes as C
+    from three_part_dwf_study_b200 import _capi as A
+
+    def e2e_step():
+        A.check(A.lib().dwf_set_gauge(d.handle, 1, C.c_void_p(th_np.ctypes.data)), d.handle)
+        infos = (A.SolveInfo * nrhs)()
+        A.check(A.lib().dwf_propagators(d.handle, nrhs, None, C.c_void_p(src_np.ctypes.data),
+                                        C.c_void_p(x_np.ctypes.data), RTOL, MAXITER,
+                                        T.SOLVER_MIXED, infos), d.handle)
+        return infos
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    e2e_total = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_total += e0.elapsed_time(e1) * 1e-3
+    barrier()
+    e2e_value = ws * nrhs * args.steps / allmax(e2e_total)
+    ref_x = x_dev.cpu().numpy().view(np.complex128)
+    e2e_agree = float(np.linalg.norm(x_np - ref_x) / np.linalg.norm(ref_x))
+
+    # ---- standalone Dslash (working set >> L2) ----
+    dslash = {}
+    peak, peak_kind = measured_peaks()
+    Dt, Dx, Dl = DSLASH_LATTICE
+    dd = T.DomainWall(Dt, Dx, Dl, M5, MF, BETA, device=local)
+    dd.set_gauge(np.random.default_rng(3).uniform(-np.pi, np.pi, 2 * Dt * Dx))
+    dstream = torch.cuda.ExternalStream(dd.stream_ptr(), device=dev)
+    for prec, dt, w in ((64, torch.float64, 8), (32, torch.float32, 4)):
+        a = torch.randn(dd.Ndof * 2, dtype=dt, device=dev)
+        b = torch.empty_like(a)
+        for _ in range(3):
+            dd.apply_dev(0, a, b)
+        dd.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record(dstream)
+        for _ in range(reps):
+            dd.apply_dev(0, a, b)
+        e1.record(dstream)
+        e1.synchronize()
+        tsec = e0.elapsed_time(e1) * 1e-3 / reps
+        gbs = dslash_bytes(Dt * Dx, Dl, w) / tsec / 1e9
+        dslash[f"complex{2 * prec}"] = {"GBs": round(gbs, 1), "frac": round(gbs / peak, 4),
+                                         "us_per_apply": round(tsec * 1e6, 2)}
+    dslash["lattice"] = list(DSLASH_LATTICE)
+    dslash["bytes_rule"] = "V*(Ls*64+32) B (FP64), V*(Ls*32+16) B (FP32) per application"
+
+    # ---- roofline of the dominant kernel (the persistent mixed solver) ----
+    V = NT * NX
+    iters = sum(i["iterations"] for infos in infos_m for i in infos)
+    rus = sum(i["reliable_updates"] for infos in infos_m for i in infos)
+    alg_bytes = iters * cg_iter_bytes(V, LS, 4) + rus * reliable_update_bytes(V, LS)
+    kernel_launch_s = kern_s / max(1, nkern)
+    achieved = alg_bytes / max(1, nkern) / kernel_launch_s / 1e9
+    traffic = None
+    tfile = REPO / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("cg_mixed_kernel_bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": "cg_mixed_kernel", "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+                "alg_bytes_per_launch": alg_bytes / max(1, nkern),
+                "kernel_ms_per_launch": kernel_launch_s * 1e3,
+                "kernel_share_of_step": kern_s / t_mixed}
+
+    line = {
+        "metric": "dwf_propagator_solves_per_s_true_res_1e-10",
+        "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_mixed_max / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (FP32 inner CG, FP64 reliable updates and true residual)",
+        "data": "synthetic (seeded hot-start links, boundary point/Z4/wall sources)",
+        "config": dict(workload_config("mixed FP32/FP64 reliable-update CG"),
+                       parallelism=f"dp{ws} (independent configurations per rank)"),
+        "plain_fp64_cg": {"value": fp64_value, "unit": "solves/s",
+                          "speedup_of_value": value / fp64_value,
+                          "iterations_mean": statistics.mean(
+                              i["iterations"] for infos in infos_f for i in infos)},
+        "iterations_mean": statistics.mean(i["iterations"] for infos in infos_m for i in infos),
+        "e2e": {"value": e2e_value, "unit": "solves/s",
+                "h2d_bytes_per_step": int(src_np.nbytes + th_np.nbytes),
+                "d2h_bytes_per_step": int(x_np.nbytes),
+                "agrees_with_device_run": e2e_agree},
+        "roofline": roofline,
+        "dslash": dslash,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        s = cpu_sample(os.cpu_count() or 1)
+        if s is not None:
+            sps, desc, _ = s
+            line["cpu_baseline"] = {"value": sps, "unit": "solves/s", "cores": os.cpu_count(),
+                                    "kind": "reference", "sample": desc}
+        else:
+            line["cpu_baseline"] = None
+    if rank == 0:
+        print(json.dumps(line))
+    d.close()
+    dd.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def calibrate_reference():
+    """Full reference solves of the 8 point sources (CPU, all cores): writes
+    oracle/bench_ref_iters.json with their iteration counts."""
+    threads = min(8, os.cpu_count() or 1)
+    res = run_ref_bench(8, threads, MAXITER)
+    if not all(res["converged"]):
+        raise SystemExit(f"reference solves did not converge: {res}")
+    REF_ITERS_FILE.write_text(json.dumps({
+        "iterations": res["iterations"], "relres": res["relres"], "rtol": RTOL,
+        "lattice": [NT, NX, LS], "M5": M5, "mf": MF, "gauge_seed": GAUGE_SEED,
+        "sources": "point, spin i%2, t_src ((i/2)%4)*Nt/4, x=0",
+        "seconds": res["seconds"], "threads": res["threads"]}, indent=1) + "\n")
+    print(REF_ITERS_FILE.read_text())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--calibrate-reference", action="store_true")
+    args = ap.parse_args()
+    if args.calibrate_reference:
+        return calibrate_reference()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return impl_reference(args)
+    return impl_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

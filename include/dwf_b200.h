@@ -90,6 +90,7 @@ typedef struct
     double true_relres;  /* FP64 |b - A x| / |b| recomputed after the solve */
     int reliable_updates;/* FP64 residual replacements (mixed path) */
     int fallback;        /* 1 if the mixed path fell back to FP64 CG */
+    double dirac_relres; /* propagator solves: |D x - src| / |src| (correlator.hpp:225-227); else 0 */
 } dwf_solve_info;
 
 typedef struct dwf_ctx dwf_ctx;
@@ -138,6 +139,26 @@ int dwf_cg(dwf_ctx* ctx, int op, int conf, const double* b, double* x, int has_g
 int dwf_cg_batch_dev(dwf_ctx* ctx, int op, int nrhs, const int* rhs_conf, const void* b_dev,
                      void* x_dev, int has_guess, double rtol, int maxiter, int solver,
                      dwf_solve_info* info);
+/* Host-buffer version of dwf_cg_batch_dev. */
+int dwf_cg_batch(dwf_ctx* ctx, int op, int nrhs, const int* rhs_conf, const double* b, double* x,
+                 int has_guess, double rtol, int maxiter, int solver, dwf_solve_info* info);
+
+/* ---- propagators -------------------------------------------------------------- */
+/* The analyzers' propagator solve for nrhs sources at once: x = (D^dag D)^-1 D^dag src,
+ * i.e. rhs = apply_D_dagger(theta, source) followed by conjugate_gradient on
+ * apply_D_dagger_D from zero (domain_wall/include/correlator.hpp:77-79, :139-142,
+ * :213-220). info[k].dirac_relres = |D x - src| / |src|. Host buffers. */
+int dwf_propagators(dwf_ctx* ctx, int nrhs, const int* rhs_conf, const double* src, double* x,
+                    double rtol, int maxiter, int solver, dwf_solve_info* info);
+/* Device-buffer version. */
+int dwf_propagators_dev(dwf_ctx* ctx, int nrhs, const int* rhs_conf, const void* src_dev,
+                        void* x_dev, double rtol, int maxiter, int solver, dwf_solve_info* info);
+
+/* Number of kernels this context has launched so far. */
+uint64_t dwf_launch_count(const dwf_ctx* ctx);
+/* Accumulated device time (ms) of the persistent solver launches, measured
+ * with CUDA events on the context stream; *nlaunch (optional) = their count. */
+double dwf_solver_kernel_ms(const dwf_ctx* ctx, uint64_t* nlaunch);
 
 #ifdef __cplusplus
 }

@@ -24,7 +24,8 @@ class DwfParams(C.Structure):
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("status", C.c_int),
                 ("solver", C.c_int), ("relres", C.c_double), ("true_relres", C.c_double),
-                ("reliable_updates", C.c_int), ("fallback", C.c_int)]
+                ("reliable_updates", C.c_int), ("fallback", C.c_int),
+                ("dirac_relres", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -50,6 +51,11 @@ SIGNATURES = {
     "dwf_apply_dev": (_I, [_P, _I, _I, _P, _P, _I, _I]),
     "dwf_cg": (_I, [_P, _I, _I, _P, _P, _I, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_cg_batch_dev": (_I, [_P, _I, _I, _P, _P, _P, _I, _D, _I, _I, C.POINTER(SolveInfo)]),
+    "dwf_cg_batch": (_I, [_P, _I, _I, _P, _P, _P, _I, _D, _I, _I, C.POINTER(SolveInfo)]),
+    "dwf_propagators": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
+    "dwf_propagators_dev": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
+    "dwf_launch_count": (C.c_uint64, [_P]),
+    "dwf_solver_kernel_ms": (C.c_double, [_P, C.POINTER(C.c_uint64)]),
 }
 
 _lib = None

@@ -52,7 +52,8 @@ int ensure_workspace(dwf_ctx* c, int nrhs)
     if ((st = grow(c, c->w_r, f)) || (st = grow(c, c->w_p, f)) || (st = grow(c, c->w_t, f)) ||
         (st = grow(c, c->w_b, f)) || (st = grow(c, c->w_x, f)) || (st = grow(c, c->w_r32, f)) ||
         (st = grow(c, c->w_p32, f)) || (st = grow(c, c->w_t32, f)) ||
-        (st = grow(c, c->w_e32, f)) || (st = grow(c, c->w_conf, size_t(nrhs))) ||
+        (st = grow(c, c->w_e32, f)) || (st = grow(c, c->w_src, f)) ||
+        (st = grow(c, c->w_conf, size_t(nrhs))) ||
         (st = grow(c, c->w_active, size_t(nrhs))) || (st = grow(c, c->w_iters, size_t(nrhs))) ||
         (st = grow(c, c->w_relres, size_t(nrhs))) || (st = grow(c, c->w_status, size_t(nrhs))) ||
         (st = grow(c, c->w_ru, size_t(nrhs))) || (st = grow(c, c->w_true, size_t(nrhs))))
@@ -127,6 +128,7 @@ int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const 
         }
     }
     CK(cudaGetLastError());
+    c->launches += two ? 2 : 1;
     return DWF_OK;
 }
 
@@ -154,6 +156,7 @@ int true_residual(dwf_ctx* c, int op, int nrhs, const int* conf_d, const double2
         residual_partials_kernel<true><<<g2, block, 0, c->stream>>>(c->L, c->w_t, b, fs, c->U64, c->usz(), conf_d, nch, ch, c->w_part);
     residual_finish_kernel<<<(nrhs + 7) / 8, 256, 0, c->stream>>>(c->w_part, nrhs, nch, c->w_true);
     CK(cudaGetLastError());
+    c->launches += 3;
     CK(cudaMemcpyAsync(out, c->w_true, nrhs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return DWF_OK;
@@ -228,7 +231,10 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     d.expected_blocks = unsigned(grid);
     CK(cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->stream));
     void* args[] = {&d};
+    CK(cudaEventRecord(c->ev0, c->stream));
     CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolverThreads), args, smem, c->stream));
+    CK(cudaEventRecord(c->ev1, c->stream));
+    c->launches += 1;
     GridBar hb{};
     iters.resize(nrhs);
     relres.resize(nrhs);
@@ -240,6 +246,10 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     CK(cudaMemcpyAsync(ru.data(), c->w_ru, nrhs * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(&hb, c->bar, sizeof(GridBar), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->solver_ms += ms;
+    c->solver_launches += 1;
     if (hb.err != 0)
         return ctx_fail(c, hb.err, hb.err == DWF_TIMEOUT ? "persistent solver: a grid barrier wait ran out"
                                                           : "persistent solver: device error");
@@ -327,9 +337,72 @@ int solve_batch(dwf_ctx* c, int op, int nrhs, const int* conf_h, const double2* 
             I.true_relres = tr[k];
             I.reliable_updates = ru[k];
             I.fallback = fallback[k];
+            I.dirac_relres = 0.0;
             if (!std::isfinite(tr[k]) && I.status == DWF_OK)
                 I.status = DWF_NONFINITE;
         }
+    }
+    return DWF_OK;
+}
+
+int dirac_residual(dwf_ctx* c, int nrhs, const int* conf_d, const double2* src,
+                   const double2* x, double* out)
+{
+    // |src - D x|^2 and |src|^2 per right-hand side
+    const int ch = 4096;
+    const int nch = (c->L.nsite + ch - 1) / ch;
+    int st = ensure_part(c, size_t(nrhs) * nch * 2);
+    if (st)
+        return st;
+    residual_partials_kernel<false><<<dim3(nch, nrhs), 256, 0, c->stream>>>(
+        c->L, x, src, c->fsz(), c->U64, c->usz(), conf_d, nch, ch, c->w_part);
+    residual_finish_kernel<<<(nrhs + 7) / 8, 256, 0, c->stream>>>(c->w_part, nrhs, nch, c->w_true);
+    CK(cudaGetLastError());
+    c->launches += 2;
+    CK(cudaMemcpyAsync(out, c->w_true, nrhs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
+                double rtol, int maxiter, int solver, dwf_solve_info* info)
+{
+    if (nrhs < 1)
+        return ctx_fail(c, DWF_BAD_ARG, "propagators: nrhs < 1");
+    if (c->nconf < 1)
+        return ctx_fail(c, DWF_BAD_ARG, "propagators: no gauge configuration (set_gauge first)");
+    for (int k = 0; conf_h && k < nrhs; ++k)
+        if (conf_h[k] < 0 || conf_h[k] >= c->nconf)
+            return ctx_fail(c, DWF_BAD_ARG, "propagators: configuration index out of range");
+    int st = ensure_workspace(c, nrhs);
+    if (st)
+        return st;
+    const long fs = c->fsz();
+    // rhs = D^dag src, per configuration, into w_b (chunks of up to 65535 fields)
+    std::vector<int> conf(nrhs, 0);
+    if (conf_h)
+        std::copy(conf_h, conf_h + nrhs, conf.begin());
+    for (int k0 = 0; k0 < nrhs; k0 += 65535)
+    {
+        const int n = std::min(65535, nrhs - k0);
+        CK(cudaMemcpyAsync(c->w_conf, conf.data() + k0, n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        st = apply_dev(c, DWF_OP_DDAG, n, c->w_conf, 0, src + k0 * fs, c->w_b + k0 * fs, 64);
+        if (st)
+            return st;
+    }
+    st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 0, rtol, maxiter, solver, 0, info);
+    if (st)
+        return st;
+    for (int k0 = 0; k0 < nrhs; k0 += 65535)
+    {
+        const int n = std::min(65535, nrhs - k0);
+        CK(cudaMemcpyAsync(c->w_conf, conf.data() + k0, n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        std::vector<double> dr(n);
+        st = dirac_residual(c, n, c->w_conf, src + k0 * fs, x + k0 * fs, dr.data());
+        if (st)
+            return st;
+        for (int k = 0; info && k < n; ++k)
+            info[k0 + k].dirac_relres = dr[k];
     }
     return DWF_OK;
 }
@@ -364,6 +437,8 @@ static int ctx_init(dwf_ctx* c, int device)
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaMalloc(&c->bar, sizeof(GridBar)));
     CK(cudaMemset(c->bar, 0, sizeof(GridBar)));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
     return DWF_OK;
 }
 
@@ -405,11 +480,15 @@ int dwf_ctx_destroy(dwf_ctx* c)
     if (c->stream)
         cudaStreamSynchronize(c->stream);
     void* bufs[] = {c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_t, c->w_b, c->w_x,
-                    c->w_r32, c->w_p32, c->w_t32, c->w_e32, c->w_part, c->w_conf, c->w_active,
+                    c->w_r32, c->w_p32, c->w_t32, c->w_e32, c->w_src, c->w_part, c->w_conf, c->w_active,
                     c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar};
     for (void* b : bufs)
         if (b)
             cudaFree(b);
+    if (c->ev0)
+        cudaEventDestroy(c->ev0);
+    if (c->ev1)
+        cudaEventDestroy(c->ev1);
     if (c->stream)
         cudaStreamDestroy(c->stream);
     delete c;
@@ -462,6 +541,7 @@ static int set_gauge_impl(dwf_ctx* c, int nconf, const double* theta, cudaMemcpy
     const int grid = int(std::min<long>((n + 255) / 256, 8L * c->nsm));
     links_kernel<<<grid, 256, 0, c->stream>>>(c->theta, n, c->U64, c->U32);
     CK(cudaGetLastError());
+    c->launches += 1;
     CK(cudaStreamSynchronize(c->stream));
     c->nconf = nconf;
     return DWF_OK;
@@ -536,6 +616,68 @@ int dwf_cg(dwf_ctx* c, int op, int conf, const double* b, double* x, int has_gue
     CK(cudaMemcpyAsync(x, c->w_x, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return info ? info->status : DWF_OK;
+}
+
+int dwf_cg_batch(dwf_ctx* c, int op, int nrhs, const int* rhs_conf, const double* b, double* x,
+                 int has_guess, double rtol, int maxiter, int solver, dwf_solve_info* info)
+{
+    if (!c || !b || !x || nrhs < 1)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    int st = ensure_workspace(c, nrhs);
+    if (st)
+        return st;
+    const size_t bytes = size_t(nrhs) * c->fsz() * sizeof(double2);
+    CK(cudaMemcpyAsync(c->w_src, b, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (has_guess)
+        CK(cudaMemcpyAsync(c->w_x, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    st = solve_batch(c, op, nrhs, rhs_conf, c->w_src, c->w_x, has_guess, rtol, maxiter, solver,
+                     c->kind == 1 ? 1 : 0, info);
+    if (st)
+        return st;
+    CK(cudaMemcpyAsync(x, c->w_x, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+int dwf_propagators_dev(dwf_ctx* c, int nrhs, const int* rhs_conf, const void* src, void* x,
+                        double rtol, int maxiter, int solver, dwf_solve_info* info)
+{
+    if (!c || !src || !x)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    return propagators(c, nrhs, rhs_conf, static_cast<const double2*>(src),
+                       static_cast<double2*>(x), rtol, maxiter, solver, info);
+}
+
+int dwf_propagators(dwf_ctx* c, int nrhs, const int* rhs_conf, const double* src, double* x,
+                    double rtol, int maxiter, int solver, dwf_solve_info* info)
+{
+    if (!c || !src || !x || nrhs < 1)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    int st = ensure_workspace(c, nrhs);
+    if (st)
+        return st;
+    const size_t bytes = size_t(nrhs) * c->fsz() * sizeof(double2);
+    CK(cudaMemcpyAsync(c->w_src, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    st = propagators(c, nrhs, rhs_conf, c->w_src, c->w_x, rtol, maxiter, solver, info);
+    if (st)
+        return st;
+    CK(cudaMemcpyAsync(x, c->w_x, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
+
+double dwf_solver_kernel_ms(const dwf_ctx* c, uint64_t* nlaunch)
+{
+    if (!c)
+        return 0.0;
+    if (nlaunch)
+        *nlaunch = c->solver_launches;
+    return c->solver_ms;
 }
 
 }  // extern "C"

@@ -18,6 +18,11 @@ struct dwf_ctx
     cudaStream_t stream = nullptr;
     uint64_t timeout_ns = 5000000000ull;
     std::string err;
+    uint64_t launches = 0;  // kernels launched by this context
+    // CUDA events bracketing each persistent solver launch on `stream`
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double solver_ms = 0.0;  // accumulated device time of solver launches
+    uint64_t solver_launches = 0;
 
     // gauge configurations
     int nconf = 0;
@@ -39,6 +44,7 @@ struct dwf_ctx
     float2* w_e32 = nullptr;
     double* w_part = nullptr;
     size_t w_part_cap = 0;
+    double2* w_src = nullptr;  // propagator sources (device staging)
     int* w_conf = nullptr;
     int* w_active = nullptr;
     int* w_iters = nullptr;
@@ -67,5 +73,8 @@ int true_residual(dwf_ctx* c, int op, int nrhs, const int* conf_d, const double2
 // out = op(in) on device fields, precision 64 or 32.
 int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const void* in,
               void* out, int precision);
+// Propagator batch: x = (D^dag D)^-1 D^dag src on device fields.
+int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
+                double rtol, int maxiter, int solver, dwf_solve_info* info);
 
 }  // namespace dwfb

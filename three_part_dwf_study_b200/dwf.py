@@ -184,6 +184,50 @@ class DomainWall:
             int(maxiter), int(solver), infos))
         return [i.as_dict() for i in infos]
 
+    def propagators(self, src, rhs_conf=None, rtol=1e-10, maxiter=10000, solver=A.SOLVER_MIXED):
+        """x = (D^dag D)^-1 D^dag src for every source (host arrays), as the
+        analyzers' propagator solves (correlator.hpp:77-79, :139-142, :213-220)."""
+        s = np.ascontiguousarray(src, dtype=np.complex128)
+        nrhs = s.size // self.Ndof
+        if nrhs < 1 or nrhs * self.Ndof != s.size:
+            raise ValueError("src: not a whole number of fields")
+        x = np.empty_like(s)
+        infos = (A.SolveInfo * nrhs)()
+        conf = None
+        if rhs_conf is not None:
+            conf = np.ascontiguousarray(rhs_conf, dtype=np.int32).reshape(-1)
+            if conf.size != nrhs:
+                raise ValueError("rhs_conf: wrong length")
+        self._check(A.lib().dwf_propagators(self._h, nrhs, _ptr(conf) if conf is not None else None,
+                                            _ptr(s), _ptr(x), float(rtol), int(maxiter),
+                                            int(solver), infos))
+        return x, [i.as_dict() for i in infos]
+
+    def propagators_dev(self, src, x, rhs_conf=None, rtol=1e-10, maxiter=10000,
+                        solver=A.SOLVER_MIXED):
+        prec, nrhs = self._dev_fields(src, "src")
+        prec2, nrhs2 = self._dev_fields(x, "x")
+        if prec != 64 or prec2 != 64 or nrhs2 != nrhs:
+            raise ValueError("src/x: expected FP64 fields of equal count")
+        infos = (A.SolveInfo * nrhs)()
+        conf = None
+        if rhs_conf is not None:
+            conf = np.ascontiguousarray(rhs_conf, dtype=np.int32).reshape(-1)
+            if conf.size != nrhs:
+                raise ValueError("rhs_conf: wrong length")
+        self._check(A.lib().dwf_propagators_dev(
+            self._h, nrhs, _ptr(conf) if conf is not None else None, C.c_void_p(src.data_ptr()),
+            C.c_void_p(x.data_ptr()), float(rtol), int(maxiter), int(solver), infos))
+        return [i.as_dict() for i in infos]
+
+    def launch_count(self):
+        return int(A.lib().dwf_launch_count(self._h))
+
+    def solver_kernel_ms(self):
+        n = C.c_uint64()
+        ms = A.lib().dwf_solver_kernel_ms(self._h, C.byref(n))
+        return ms, n.value
+
     def sync(self):
         self._check(A.lib().dwf_sync(self._h))
 

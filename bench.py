@@ -529,6 +529,21 @@ def calibrate_reference():
     print(REF_ITERS_FILE.read_text())
 
 
+def profile_case():
+    """One mixed and one FP64 propagator batch of the workload (for ncu)."""
+    import torch
+    import three_part_dwf_study_b200 as T
+    d = T.DomainWall(NT, NX, LS, M5, MF, BETA)
+    d.set_gauge(workload_gauge(0))
+    src = torch.from_numpy(workload_sources(0).view(np.float64).copy()).cuda()
+    x = torch.zeros_like(src)
+    for solver in (T.SOLVER_MIXED, T.SOLVER_CG64):
+        infos = d.propagators_dev(src, x, rtol=RTOL, maxiter=MAXITER, solver=solver)
+        assert all(i["converged"] for i in infos)
+    d.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -537,7 +552,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
+    ap.add_argument("--profile-case", action="store_true")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case()
     if args.calibrate_reference:
         return calibrate_reference()
     if args.warmup < 3 and args.impl == "ours":

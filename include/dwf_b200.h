@@ -154,6 +154,84 @@ int dwf_propagators(dwf_ctx* ctx, int nrhs, const int* rhs_conf, const double* s
 int dwf_propagators_dev(dwf_ctx* ctx, int nrhs, const int* rhs_conf, const void* src_dev,
                         void* x_dev, double rtol, int maxiter, int solver, dwf_solve_info* info);
 
+/* ---- HMC ------------------------------------------------------------------ */
+/* Leapfrog parameters. Domain wall: epsilon = dwf.epsilon, steps =
+ * dwf.leapfrog_steps, rtol/maxiter = dwf.pseudofermion_rtol/_maxiter.
+ * Wilson: epsilon = wilson.trajectory_length / wilson.hmc_steps, steps =
+ * wilson.hmc_steps, rtol/maxiter = wilson.force_cg_tolerance/_max_iterations. */
+typedef struct
+{
+    double epsilon;
+    int steps;
+    double rtol;
+    int maxiter;
+    int solver; /* dwf_solver used for the pseudofermion solves */
+} dwf_hmc_params;
+
+typedef struct
+{
+    double dH, H0, H;        /* Hamiltonian change, initial and final (FP64) */
+    double S_gauge, S_pf;    /* actions at the final configuration */
+    double kinetic0, kinetic;
+    double plaquette;        /* average plaquette: proposal (domain wall), result (Wilson) */
+    double acceptance_probability; /* min(1, exp(-dH)) */
+    int accepted;            /* Wilson only: u < acceptance_probability */
+    int solves;              /* pseudofermion solves performed */
+    long cg_iterations;      /* summed over those solves */
+    int status;
+} dwf_traj_info;
+
+/* Gauge action beta sum(1 - cos P) and force on host theta
+ * (gauge_action_force, domain_wall/include/gauge.hpp:26-62; wilson/include/gauge.hpp:38-62).
+ * Uses the context's beta. force: host double[2*Nt*Nx] or NULL. */
+int dwf_gauge_action_force(dwf_ctx* ctx, const double* theta, double* action, double* force);
+/* average_plaquette (domain_wall/include/gauge.hpp:64-73; wilson/include/gauge.hpp:29-36). */
+int dwf_average_plaquette(dwf_ctx* ctx, const double* theta, double* plaquette);
+/* Pseudofermion action S = Re<phi, eta>, eta = (D D^dag)^-1 phi, and its force
+ * (pseudofermion_action_force, domain_wall/include/pseudofermion.hpp:22-166;
+ * wilson/include/gauge.hpp:68-122). eta_guess may be NULL (domain wall warm start;
+ * Wilson always starts from zero). force, eta_out may be NULL. */
+int dwf_pf_action_force(dwf_ctx* ctx, const double* theta, const double* phi,
+                        const double* eta_guess, double rtol, int maxiter, int solver,
+                        double* action, double* force, double* eta_out, dwf_solve_info* info);
+/* One domain-wall HMC trajectory from theta0 with the heat-bath draws chi
+ * (Ndof complex) and mom (2*Nt*Nx) supplied by the caller: phi = D chi, leapfrog,
+ * proposal in theta_out, dH in info (domain_wall/generate_configs.cpp:56-160).
+ * The Metropolis test (:158-169) is the caller's, with its own uniform draw. */
+int dwf_hmc_trajectory(dwf_ctx* ctx, const dwf_hmc_params* hp, const double* theta0,
+                       const double* chi, const double* mom, double* theta_out,
+                       dwf_traj_info* info);
+
+/* ---- Wilson ------------------------------------------------------------------ */
+/* Wilson context: parameters.txt keys wilson.Nt, wilson.Nx, wilson.m0, wilson.beta,
+ * wilson.time_boundary_sign, wilson.space_boundary_sign
+ * (wilson/include/parameters.hpp:6-27). The context works with every dwf_*
+ * entry point above (operators act on Wilson fields, Ls = 1); its solves use
+ * the stopping rule of the reference's Eigen ConjugateGradient,
+ * |r|^2 < tol^2 |b|^2 (wilson/include/cg_solver.hpp:24-31). */
+typedef struct
+{
+    int Nt, Nx;
+    double m0, beta;
+    double bc_t, bc_x;
+    int device;
+} wil_params;
+
+int wil_ctx_create(const wil_params* params, dwf_ctx** out);
+/* solve_CGNR (wilson/include/cg_solver.hpp:19-51). info3 = {iterations, normal
+ * residual, Dirac residual}; DWF_NOT_CONVERGED (with the reference's message in
+ * dwf_last_error) when the normal residual exceeds 20 tol. */
+int wil_solve_cgnr(dwf_ctx* ctx, const double* theta, const double* source, double tol,
+                   int maxiter, int solver, double* x, double* info3);
+/* solve_DDdag (wilson/include/cg_solver.hpp:53-78). */
+int wil_solve_dddag(dwf_ctx* ctx, const double* theta, const double* phi, double tol, int maxiter,
+                    int solver, double* eta, double* residual);
+/* hmc_step (wilson/include/gauge.hpp:124-180) with mom, chi and the uniform u
+ * drawn by the caller (order: mom, chi, u). theta_out = accepted ? new : old. */
+int wil_hmc_step(dwf_ctx* ctx, const dwf_hmc_params* hp, const double* theta_old,
+                 const double* mom, const double* chi, double u, double* theta_out,
+                 dwf_traj_info* info);
+
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);
 /* Accumulated device time (ms) of the persistent solver launches, measured

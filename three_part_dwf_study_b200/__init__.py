@@ -8,6 +8,7 @@ from . import _capi
 from ._capi import (OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD, SOLVER_CG64, SOLVER_MIXED, DwfError,
                     LIB_PATH)
 from .dwf import DomainWall, CgResult
+from .wilson import Wilson
 
-__all__ = ["DomainWall", "CgResult", "DwfError", "OP_D", "OP_DDAG", "OP_DDDAG", "OP_DDAGD",
+__all__ = ["DomainWall", "Wilson", "CgResult", "DwfError", "OP_D", "OP_DDAG", "OP_DDDAG", "OP_DDAGD",
            "SOLVER_CG64", "SOLVER_MIXED", "LIB_PATH"]

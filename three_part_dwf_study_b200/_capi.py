@@ -31,6 +31,27 @@ class SolveInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class HmcParams(C.Structure):
+    _fields_ = [("epsilon", C.c_double), ("steps", C.c_int), ("rtol", C.c_double),
+                ("maxiter", C.c_int), ("solver", C.c_int)]
+
+
+class TrajInfo(C.Structure):
+    _fields_ = [("dH", C.c_double), ("H0", C.c_double), ("H", C.c_double),
+                ("S_gauge", C.c_double), ("S_pf", C.c_double), ("kinetic0", C.c_double),
+                ("kinetic", C.c_double), ("plaquette", C.c_double),
+                ("acceptance_probability", C.c_double), ("accepted", C.c_int),
+                ("solves", C.c_int), ("cg_iterations", C.c_long), ("status", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class WilParams(C.Structure):
+    _fields_ = [("Nt", C.c_int), ("Nx", C.c_int), ("m0", C.c_double), ("beta", C.c_double),
+                ("bc_t", C.c_double), ("bc_x", C.c_double), ("device", C.c_int)]
+
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -55,6 +76,14 @@ SIGNATURES = {
     "dwf_propagators": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_propagators_dev": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_launch_count": (C.c_uint64, [_P]),
+    "dwf_gauge_action_force": (_I, [_P, _P, _P, _P]),
+    "dwf_average_plaquette": (_I, [_P, _P, _P]),
+    "dwf_pf_action_force": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _P, _P, C.POINTER(SolveInfo)]),
+    "dwf_hmc_trajectory": (_I, [_P, C.POINTER(HmcParams), _P, _P, _P, _P, C.POINTER(TrajInfo)]),
+    "wil_ctx_create": (_I, [C.POINTER(WilParams), C.POINTER(_P)]),
+    "wil_solve_cgnr": (_I, [_P, _P, _P, _D, _I, _I, _P, _P]),
+    "wil_solve_dddag": (_I, [_P, _P, _P, _D, _I, _I, _P, _P]),
+    "wil_hmc_step": (_I, [_P, C.POINTER(HmcParams), _P, _P, _P, _D, _P, C.POINTER(TrajInfo)]),
     "dwf_solver_kernel_ms": (C.c_double, [_P, C.POINTER(C.c_uint64)]),
 }
 

@@ -390,7 +390,8 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
         if (st)
             return st;
     }
-    st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 0, rtol, maxiter, solver, 0, info);
+    st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 0, rtol, maxiter, solver,
+                     c->kind == 1 ? 1 : 0, info);
     if (st)
         return st;
     for (int k0 = 0; k0 < nrhs; k0 += 65535)
@@ -429,7 +430,7 @@ const char* dwf_status_string(int s)
     }
 }
 
-static int ctx_init(dwf_ctx* c, int device)
+int dwfb_ctx_init(dwf_ctx* c, int device)
 {
     c->device = device;
     CK(cudaSetDevice(device));
@@ -462,7 +463,7 @@ int dwf_ctx_create(const dwf_params* p, dwf_ctx** out)
     c->L.bcx = 1.0;
     c->L.fifth = 1;
     c->beta = p->beta;
-    const int st = ctx_init(c, p->device);
+    const int st = dwfb_ctx_init(c, p->device);
     if (st)
     {
         dwf_ctx_destroy(c);
@@ -479,7 +480,8 @@ int dwf_ctx_destroy(dwf_ctx* c)
     cudaSetDevice(c->device);
     if (c->stream)
         cudaStreamSynchronize(c->stream);
-    void* bufs[] = {c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_t, c->w_b, c->w_x,
+    void* bufs[] = {c->h_mom, c->h_force, c->h_part, c->h_scal, c->h_chi, c->h_phi, c->h_eta,
+                    c->h_xi, c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_t, c->w_b, c->w_x,
                     c->w_r32, c->w_p32, c->w_t32, c->w_e32, c->w_src, c->w_part, c->w_conf, c->w_active,
                     c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar};
     for (void* b : bufs)
@@ -516,7 +518,10 @@ int dwf_sync(dwf_ctx* c)
 
 void* dwf_stream(dwf_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
 
-static int set_gauge_impl(dwf_ctx* c, int nconf, const double* theta, cudaMemcpyKind kind)
+}  // extern "C"
+
+namespace dwfb {
+int set_gauge(dwf_ctx* c, int nconf, const double* theta, cudaMemcpyKind kind)
 {
     if (!c || nconf < 1 || !theta)
         return DWF_BAD_ARG;
@@ -546,15 +551,18 @@ static int set_gauge_impl(dwf_ctx* c, int nconf, const double* theta, cudaMemcpy
     c->nconf = nconf;
     return DWF_OK;
 }
+}  // namespace dwfb
+
+extern "C" {
 
 int dwf_set_gauge(dwf_ctx* c, int nconf, const double* theta)
 {
-    return set_gauge_impl(c, nconf, theta, cudaMemcpyHostToDevice);
+    return set_gauge(c, nconf, theta, cudaMemcpyHostToDevice);
 }
 
 int dwf_set_gauge_dev(dwf_ctx* c, int nconf, const double* theta_dev)
 {
-    return set_gauge_impl(c, nconf, theta_dev, cudaMemcpyDeviceToDevice);
+    return set_gauge(c, nconf, theta_dev, cudaMemcpyDeviceToDevice);
 }
 
 int dwf_apply_dev(dwf_ctx* c, int op, int conf, const void* in, void* out, int nrhs, int precision)

@@ -54,9 +54,22 @@ struct dwf_ctx
     double* w_true = nullptr;
     dwfb::GridBar* bar = nullptr;
 
+    // HMC workspace (allocated on first use)
+    double* h_mom = nullptr;    // [2V]
+    double* h_force = nullptr;  // [2V]
+    double* h_part = nullptr;   // [2 * kRedBlocks]
+    double* h_scal = nullptr;   // [16]
+    double2* h_chi = nullptr;   // [fsz]
+    double2* h_phi = nullptr;
+    double2* h_eta = nullptr;
+    double2* h_xi = nullptr;
+
     long fsz() const { return 2L * L.nsite; }
     long usz() const { return 2L * L.V; }
 };
+
+// Device selection, stream, barrier state and events of a new context.
+extern "C" int dwfb_ctx_init(dwf_ctx* c, int device);
 
 namespace dwfb {
 
@@ -73,6 +86,8 @@ int true_residual(dwf_ctx* c, int op, int nrhs, const int* conf_d, const double2
 // out = op(in) on device fields, precision 64 or 32.
 int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const void* in,
               void* out, int precision);
+// Upload nconf configurations (host or device pointer) and recompute links.
+int set_gauge(dwf_ctx* c, int nconf, const double* theta, cudaMemcpyKind kind);
 // Propagator batch: x = (D^dag D)^-1 D^dag src on device fields.
 int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
                 double rtol, int maxiter, int solver, dwf_solve_info* info);

@@ -220,6 +220,61 @@ class DomainWall:
             C.c_void_p(x.data_ptr()), float(rtol), int(maxiter), int(solver), infos))
         return [i.as_dict() for i in infos]
 
+    # ---- HMC pieces (reference names) -----------------------------------------------
+    def gauge_action_force(self, theta):
+        """(action, force) -- domain_wall/include/gauge.hpp:26-62."""
+        th = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+        self._theta = None
+        a = C.c_double()
+        f = np.empty(self.Ngauge)
+        self._check(A.lib().dwf_gauge_action_force(self._h, _ptr(th), C.byref(a), _ptr(f)))
+        return a.value, f
+
+    def average_plaquette(self, theta):
+        th = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+        self._theta = None
+        p = C.c_double()
+        self._check(A.lib().dwf_average_plaquette(self._h, _ptr(th), C.byref(p)))
+        return p.value
+
+    def pseudofermion_action_force(self, theta, phi, eta_guess=None, rtol=1e-10, maxiter=1000,
+                                   solver=A.SOLVER_CG64):
+        """dict(action, force, eta, iterations, relative_residual) --
+        domain_wall/include/pseudofermion.hpp:22-166 (raises where it throws)."""
+        th = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+        self._theta = None
+        ph = np.ascontiguousarray(phi, dtype=np.complex128)
+        g = np.ascontiguousarray(eta_guess, dtype=np.complex128) if eta_guess is not None else None
+        a = C.c_double()
+        f = np.empty(self.Ngauge)
+        eta = np.empty(self.Ndof, np.complex128)
+        info = A.SolveInfo()
+        st = A.lib().dwf_pf_action_force(self._h, _ptr(th), _ptr(ph),
+                                          _ptr(g) if g is not None else None, float(rtol),
+                                          int(maxiter), int(solver), C.byref(a), _ptr(f),
+                                          _ptr(eta), C.byref(info))
+        if st != A.DWF_OK:
+            raise RuntimeError(A.lib().dwf_last_error(self._h).decode() or A.status_string(st))
+        return dict(action=a.value, force=f, eta=eta, iterations=info.iterations,
+                    relative_residual=info.relres, info=info.as_dict())
+
+    def hmc_trajectory(self, theta0, chi, mom, epsilon, steps, rtol=1e-10, maxiter=1000,
+                       solver=A.SOLVER_CG64):
+        """Proposal and trajectory report for one domain-wall trajectory
+        (domain_wall/generate_configs.cpp:56-160); Metropolis is the caller's."""
+        th = np.ascontiguousarray(theta0, dtype=np.float64).reshape(-1)
+        self._theta = None
+        ch = np.ascontiguousarray(chi, dtype=np.complex128)
+        mo = np.ascontiguousarray(mom, dtype=np.float64)
+        out = np.empty(self.Ngauge)
+        hp = A.HmcParams(float(epsilon), int(steps), float(rtol), int(maxiter), int(solver))
+        info = A.TrajInfo()
+        st = A.lib().dwf_hmc_trajectory(self._h, C.byref(hp), _ptr(th), _ptr(ch), _ptr(mo),
+                                         _ptr(out), C.byref(info))
+        if st != A.DWF_OK:
+            raise RuntimeError(A.lib().dwf_last_error(self._h).decode() or A.status_string(st))
+        return out, info.as_dict()
+
     def launch_count(self):
         return int(A.lib().dwf_launch_count(self._h))
 

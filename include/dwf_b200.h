@@ -232,6 +232,61 @@ int wil_hmc_step(dwf_ctx* ctx, const dwf_hmc_params* hp, const double* theta_old
                  const double* mom, const double* chi, double u, double* theta_out,
                  dwf_traj_info* info);
 
+/* ---- measurements ------------------------------------------------------------ */
+/* Per-configuration source set: boundary point sources at x = 0 and boundary
+ * wall sources, each at source times t_k = k*Nt/n (k < n) for both source
+ * spins, and n_noise complex Z4 boundary-noise vectors. n_point_times =
+ * n_wall_times = 2 gives the reference's {0, Nt/2}
+ * (domain_wall/include/correlator.hpp:120, :251). */
+typedef struct
+{
+    int n_point_times;
+    int n_wall_times;
+    int n_noise;      /* eta.noise_vectors */
+    int max_momentum; /* analysis.max_momentum (0..Nx/2, at most 15) */
+    double rtol;      /* dwf.propagator_rtol */
+    int maxiter;      /* dwf.propagator_maxiter */
+    int solver;       /* dwf_solver */
+} dwf_measure_params;
+
+/* All propagators of nconf configurations in one batched solve, then the
+ * contractions (domain_wall/include/correlator.hpp:27-310):
+ *   cpp, cj5 : [nconf][Nt]  C_PP and C_J5 from the wall sources (compute_CPP_CJ5)
+ *   loop     : [nconf][Nt*Nx] complex, the Z4 loop density
+ *              (estimate_pseudoscalar_loop_density)
+ *   mom_cpp  : [nconf][max_momentum+1][Nt] from the point sources (compute_momentum_CPP)
+ * z4: [nconf][n_noise][Nt][Nx][2] digits 0..3 drawn by the caller in the
+ * reference's order (dwf_z4_digits with seed eta.random_seed + 104729*config,
+ * domain_wall/analyze_configs.cpp:66-68). Output pointers may be NULL.
+ * info: [nconf * (2*n_point_times + 2*n_wall_times + n_noise)] or NULL,
+ * right-hand sides ordered point, wall, noise within each configuration. */
+int dwf_measure(dwf_ctx* ctx, const dwf_measure_params* mp, int nconf, const double* thetas,
+                const signed char* z4, double* cpp, double* cj5, double* loop, double* mom_cpp,
+                dwf_solve_info* info);
+/* pseudoscalar_correlator (wilson/include/correlator.hpp:10-40) for nconf
+ * configurations: corr [nconf][Nt]. DWF_NOT_CONVERGED (reference message in
+ * dwf_last_error) if any solve misses the 20*tol check of solve_CGNR.
+ * info: [2*nconf] or NULL. */
+int wil_pseudoscalar_correlator(dwf_ctx* ctx, int nconf, const double* thetas, int src_t,
+                                int src_x, double tol, int maxiter, int solver, double* corr,
+                                dwf_solve_info* info);
+
+/* ---- host random streams ----------------------------------------------------- */
+/* The reference draws from std::mt19937_64 with std::normal_distribution<double>,
+ * std::uniform_real_distribution<double>(0, 1) (domain_wall/generate_configs.cpp:23-25,
+ * wilson/include/gauge.hpp:16-18) and std::uniform_int_distribution<int>(0, 3)
+ * (domain_wall/include/correlator.hpp:35-36); these reproduce those streams. */
+typedef struct dwf_rng dwf_rng;
+int dwf_rng_create(uint64_t seed, dwf_rng** out);
+int dwf_rng_destroy(dwf_rng* rng);
+int dwf_rng_normals(dwf_rng* rng, long n, double* out);
+int dwf_rng_uniform(dwf_rng* rng, double* out);
+/* n complex entries Complex(normal, normal)/sqrt(2), imaginary part drawn
+ * first, as the reference's chi (generate_configs.cpp:58-62, gauge.hpp:138-140). */
+int dwf_rng_pseudofermion(dwf_rng* rng, long n, double* chi);
+/* n Z4 digits from mt19937_64(seed) (correlator.hpp:35-58). */
+int dwf_z4_digits(uint64_t seed, long n, signed char* out);
+
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);
 /* Accumulated device time (ms) of the persistent solver launches, measured

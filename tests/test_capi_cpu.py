@@ -71,3 +71,28 @@ def test_parameters_reader_semantics(tmp_path):
     ok = TextConfig(text="a = 1.5e-3 # x\nb = -2\n")
     assert ok.real("a") == 1.5e-3 and ok.integer("b") == -2
     assert ok.unsigned_integer("b") == (1 << 64) - 2
+
+
+def test_host_random_streams_match_reference_draws():
+    """The product's host RNG reproduces the reference's streams (pinned by the
+    known answers and by the oracle, which the reference's own HMC runs pin)."""
+    import numpy as np
+    from oracle import oracle as O
+    from three_part_dwf_study_b200.rng import Rng, z4_digits
+
+    assert Rng(1234).normals(2).tolist() == [0.20515413959099182, -0.33619173225969745]
+    assert z4_digits(918273, 8).tolist() == [1, 0, 2, 1, 1, 3, 1, 0]
+    ndof, ng = 64, 32
+    chi, mom, u = O.dwf_draws(77, 2, ndof, ng)
+    r = Rng(77)
+    for k in range(2):   # domain wall order: chi, mom, u
+        assert np.array_equal(r.pseudofermion(ndof), chi[k])
+        assert np.array_equal(r.normals(ng), mom[k])
+        assert r.uniform() == u[k]
+    mom, chi, u = O.wil_draws(78, 2, ndof, ng)
+    r = Rng(78)
+    for k in range(2):   # Wilson order: mom, chi, u
+        assert np.array_equal(r.normals(ng), mom[k])
+        assert np.array_equal(r.pseudofermion(ndof), chi[k])
+        assert r.uniform() == u[k]
+    assert np.array_equal(z4_digits(5, 1000), O.rng_z4(5, 1000))

@@ -52,6 +52,12 @@ class WilParams(C.Structure):
                 ("bc_t", C.c_double), ("bc_x", C.c_double), ("device", C.c_int)]
 
 
+class MeasureParams(C.Structure):
+    _fields_ = [("n_point_times", C.c_int), ("n_wall_times", C.c_int), ("n_noise", C.c_int),
+                ("max_momentum", C.c_int), ("rtol", C.c_double), ("maxiter", C.c_int),
+                ("solver", C.c_int)]
+
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -76,6 +82,16 @@ SIGNATURES = {
     "dwf_propagators": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_propagators_dev": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_launch_count": (C.c_uint64, [_P]),
+    "dwf_measure": (_I, [_P, C.POINTER(MeasureParams), _I, _P, _P, _P, _P, _P, _P,
+                         C.POINTER(SolveInfo)]),
+    "wil_pseudoscalar_correlator": (_I, [_P, _I, _P, _I, _I, _D, _I, _I, _P,
+                                         C.POINTER(SolveInfo)]),
+    "dwf_rng_create": (_I, [C.c_uint64, C.POINTER(_P)]),
+    "dwf_rng_destroy": (_I, [_P]),
+    "dwf_rng_normals": (_I, [_P, C.c_long, _P]),
+    "dwf_rng_uniform": (_I, [_P, C.POINTER(C.c_double)]),
+    "dwf_rng_pseudofermion": (_I, [_P, C.c_long, _P]),
+    "dwf_z4_digits": (_I, [C.c_uint64, C.c_long, _P]),
     "dwf_gauge_action_force": (_I, [_P, _P, _P, _P]),
     "dwf_average_plaquette": (_I, [_P, _P, _P]),
     "dwf_pf_action_force": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _P, _P, C.POINTER(SolveInfo)]),

@@ -275,6 +275,39 @@ class DomainWall:
             raise RuntimeError(A.lib().dwf_last_error(self._h).decode() or A.status_string(st))
         return out, info.as_dict()
 
+    # ---- measurements ---------------------------------------------------------------
+    def measure(self, thetas, z4=None, n_point_times=2, n_wall_times=2, n_noise=0,
+                max_momentum=0, rtol=1e-8, maxiter=800, solver=A.SOLVER_MIXED):
+        """Batched propagators and contractions for every configuration
+        (domain_wall/include/correlator.hpp:27-310). Returns dict of
+        cpp, cj5 [nconf, Nt], loop [nconf, Nt*Nx] complex, mom_cpp
+        [nconf, max_momentum+1, Nt] and the per-right-hand-side solve reports."""
+        th = np.ascontiguousarray(thetas, dtype=np.float64).reshape(-1, self.Ngauge)
+        nconf = th.shape[0]
+        self._theta = None
+        V = self.Nt * self.Nx
+        zz = None
+        if n_noise > 0:
+            zz = np.ascontiguousarray(z4, dtype=np.int8).reshape(-1)
+            if zz.size != nconf * n_noise * V * 2:
+                raise ValueError("z4: expected nconf*n_noise*Nt*Nx*2 digits")
+        mp = A.MeasureParams(int(n_point_times), int(n_wall_times), int(n_noise),
+                             int(max_momentum), float(rtol), int(maxiter), int(solver))
+        cpp = np.zeros((nconf, self.Nt))
+        cj5 = np.zeros((nconf, self.Nt))
+        loop = np.zeros((nconf, V), np.complex128)
+        nmom = max_momentum + 1 if n_point_times > 0 else 0
+        mom = np.zeros((nconf, max(nmom, 1), self.Nt))
+        R = 2 * n_point_times + 2 * n_wall_times + n_noise
+        infos = (A.SolveInfo * (nconf * R))()
+        st = A.lib().dwf_measure(self._h, C.byref(mp), nconf, _ptr(th),
+                                 _ptr(zz) if zz is not None else None, _ptr(cpp), _ptr(cj5),
+                                 _ptr(loop), _ptr(mom), infos)
+        if st != A.DWF_OK:
+            raise RuntimeError(A.lib().dwf_last_error(self._h).decode() or A.status_string(st))
+        return dict(cpp=cpp, cj5=cj5, loop=loop, mom_cpp=mom[:, :nmom],
+                    info=[i.as_dict() for i in infos])
+
     def launch_count(self):
         return int(A.lib().dwf_launch_count(self._h))
 

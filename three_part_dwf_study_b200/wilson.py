@@ -84,3 +84,19 @@ class Wilson(DomainWall):
         if st != A.DWF_OK:
             self._raise(st)
         return out, info.as_dict()
+
+    def pseudoscalar_correlator(self, thetas, source_t, source_x, tolerance, max_iterations,
+                                solver=A.SOLVER_CG64):
+        """C(t) per configuration [nconf, Nt] (wilson/include/correlator.hpp:10-40)."""
+        th = np.ascontiguousarray(thetas, dtype=np.float64).reshape(-1, self.Ngauge)
+        self._theta = None
+        nconf = th.shape[0]
+        corr = np.zeros((nconf, self.Nt))
+        infos = (A.SolveInfo * (2 * nconf))()
+        st = A.lib().wil_pseudoscalar_correlator(self._h, nconf, _ptr(th), int(source_t),
+                                                 int(source_x), float(tolerance),
+                                                 int(max_iterations), int(solver), _ptr(corr),
+                                                 infos)
+        if st != A.DWF_OK:
+            self._raise(st)
+        return corr

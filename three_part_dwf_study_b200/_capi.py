@@ -4,10 +4,12 @@ The library is required: importing a compute entry point without it raises,
 there is no CPU fallback.
 """
 import ctypes as C
+import os
 from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "_lib" / "libdwfb200.so"
+# DWF_B200_LIB selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = Path(os.environ.get("DWF_B200_LIB", _PKG / "_lib" / "libdwfb200.so"))
 
 DWF_OK, DWF_NOT_CONVERGED, DWF_ZERO_DENOM, DWF_NONFINITE = 0, 1, 2, 3
 DWF_CUDA_ERROR, DWF_TIMEOUT, DWF_BAD_ARG = 4, 5, 6

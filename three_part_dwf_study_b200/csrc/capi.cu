@@ -49,7 +49,8 @@ int ensure_workspace(dwf_ctx* c, int nrhs)
     CK(cudaStreamSynchronize(c->stream));
     const size_t f = size_t(nrhs) * c->fsz();
     int st;
-    if ((st = grow(c, c->w_r, f)) || (st = grow(c, c->w_p, f)) || (st = grow(c, c->w_t, f)) ||
+    if ((st = grow(c, c->w_r, f)) || (st = grow(c, c->w_p, f)) || (st = grow(c, c->w_p2, f)) ||
+        (st = grow(c, c->w_t, f)) || (st = grow(c, c->w_p32b, f)) ||
         (st = grow(c, c->w_b, f)) || (st = grow(c, c->w_x, f)) || (st = grow(c, c->w_r32, f)) ||
         (st = grow(c, c->w_p32, f)) || (st = grow(c, c->w_t32, f)) ||
         (st = grow(c, c->w_e32, f)) || (st = grow(c, c->w_src, f)) ||
@@ -186,9 +187,11 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     d.x = x;
     d.r = c->w_r;
     d.p = c->w_p;
+    d.p2 = c->w_p2;
     d.t = c->w_t;
     d.r32 = c->w_r32;
     d.p32 = c->w_p32;
+    d.p32b = c->w_p32b;
     d.t32 = c->w_t32;
     d.e32 = c->w_e32;
     d.rtol = rtol;
@@ -205,8 +208,12 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     d.bar = c->bar;
     d.timeout_ns = c->timeout_ns;
 
-    const void* fn = mixed ? reinterpret_cast<const void*>(&cg_mixed_kernel)
-                           : reinterpret_cast<const void*>(&cg64_kernel);
+    // single right-hand side: fused two-barrier iteration; batches: three barriers
+    const bool single = nrhs == 1;
+    const void* fn = mixed ? (single ? reinterpret_cast<const void*>(&cg_mixed_kernel<true, 2>)
+                                     : reinterpret_cast<const void*>(&cg_mixed_kernel<false, 3>))
+                           : (single ? reinterpret_cast<const void*>(&cg64_kernel<true, 2>)
+                                     : reinterpret_cast<const void*>(&cg64_kernel<false, 3>));
     const size_t smem = solver_smem_bytes(nrhs);
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int bps = 0;
@@ -214,20 +221,37 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     if (bps < 1)
         return ctx_fail(c, DWF_CUDA_ERROR, "solver kernel cannot be resident");
     const int cap = bps * c->nsm;
-    // chunking: aim at about two units per block
-    const long total = long(nrhs) * c->L.nsite;
-    long ch = (total + 2L * cap - 1) / (2L * cap);
-    ch = ((ch + kSolverThreads - 1) / kSolverThreads) * kSolverThreads;
-    ch = std::max<long>(ch, kSolverThreads);
-    const long nsite_r = ((c->L.nsite + kSolverThreads - 1) / kSolverThreads) * kSolverThreads;
-    ch = std::min(ch, nsite_r);
-    d.ch = int(ch);
-    d.nch = int((c->L.nsite + ch - 1) / ch);
-    int st = ensure_part(c, size_t(nrhs) * d.nch * 2);
+    // Work units = (right-hand side, chunk). Pick the chunk count that fills
+    // the resident blocks in whole waves (every block gets the same number of
+    // units, up to one), preferring fewer, larger chunks.
+    const int nsite = c->L.nsite;
+    int best_nch = 1, best_waves = 1;
+    double best_eff = -1.0;
+    for (int nch = 1; nch <= 4096; ++nch)
+    {
+        const long ch_try = (nsite + nch - 1) / nch;
+        if (nch > 1 && ch_try < kSolverThreads / 2)
+            break;
+        const long u = long(nrhs) * nch;
+        const long waves = (u + cap - 1) / cap;
+        const double eff = double(u) / double(waves * cap);
+        if (eff > best_eff + 0.02)
+        {
+            best_eff = eff;
+            best_nch = nch;
+            best_waves = int(waves);
+        }
+        if (eff >= 0.95)
+            break;
+    }
+    d.nch = best_nch;
+    d.ch = (nsite + best_nch - 1) / best_nch;
+    const long units = long(nrhs) * d.nch;
+    int st = ensure_part(c, size_t(units) * 2);
     if (st)
         return st;
     d.part = c->w_part;
-    const int grid = int(std::min<long>(cap, long(nrhs) * d.nch));
+    const int grid = int(std::min<long>(cap, (units + best_waves - 1) / best_waves));
     d.expected_blocks = unsigned(grid);
     CK(cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->stream));
     void* args[] = {&d};
@@ -481,7 +505,7 @@ int dwf_ctx_destroy(dwf_ctx* c)
     if (c->stream)
         cudaStreamSynchronize(c->stream);
     void* bufs[] = {c->h_mom, c->h_force, c->h_part, c->h_scal, c->h_chi, c->h_phi, c->h_eta,
-                    c->h_xi, c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_t, c->w_b, c->w_x,
+                    c->h_xi, c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_p2, c->w_p32b, c->w_t, c->w_b, c->w_x,
                     c->w_r32, c->w_p32, c->w_t32, c->w_e32, c->w_src, c->w_part, c->w_conf, c->w_active,
                     c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar};
     for (void* b : bufs)

@@ -35,11 +35,13 @@ struct dwf_ctx
     int ws_rhs = 0;
     double2* w_r = nullptr;
     double2* w_p = nullptr;
+    double2* w_p2 = nullptr;
     double2* w_t = nullptr;
     double2* w_b = nullptr;  // host-pointer entry points stage b / in here
     double2* w_x = nullptr;  // and x / out here
     float2* w_r32 = nullptr;
     float2* w_p32 = nullptr;
+    float2* w_p32b = nullptr;
     float2* w_t32 = nullptr;
     float2* w_e32 = nullptr;
     double* w_part = nullptr;

@@ -11,10 +11,14 @@
 //
 // Reference algorithm (DWF_SOLVER_CG64): domain_wall/include/cg_solver.hpp:17-64.
 // Per iteration, with A = D2 D1 (D1 = D for D^dag D, D^dag for D D^dag):
-//   phase 1: t = D1 p,  |t|^2 = <p, A p>                  | grid barrier
+//   phase 1: p = r + beta p_old (formed on the fly at every stencil point and
+//            stored at the centre into the other direction buffer),
+//            t = D1 p, |t|^2 = <p, A p>                     | grid barrier
 //   phase 2: x += alpha p, r -= alpha D2 t, |r|^2           | grid barrier
-//   phase 3: p = r + beta p                                 | grid barrier
+// The direction is double-buffered so that phase 1 reads p_old and r at the
+// neighbours while it writes the new p, with no third barrier.
 #include "solver.cuh"
+
 
 namespace dwfb {
 namespace {
@@ -24,7 +28,8 @@ struct Smem
     double* scratch;  // 64 doubles
     double* rr;       // |r|^2 per right-hand side
     double* bb;       // |b|^2
-    double* cf;       // alpha, then beta
+    double* cf;       // beta
+    double* al;       // alpha
     double* aux;      // reduction target
     double* rru;      // |r|^2 at the last reliable update (mixed)
     int* state;       // RHS_ACTIVE or the final dwf_status
@@ -42,7 +47,8 @@ __device__ Smem carve(int nrhs)
     s.rr = sm + 64;
     s.bb = s.rr + nrhs;
     s.cf = s.bb + nrhs;
-    s.aux = s.cf + nrhs;
+    s.al = s.cf + nrhs;
+    s.aux = s.al + nrhs;
     s.rru = s.aux + nrhs;
     int* ib = reinterpret_cast<int*>(s.rru + nrhs);
     s.state = ib;
@@ -114,10 +120,11 @@ __device__ void sweep(const SolveDesc& d, const int* act, int nact, double* scra
         const int k = u / d.nch, c = u - k * d.nch, j = act[k];
         const int beg = c * d.ch;
         const int end = min(beg + d.ch, d.L.nsite);
+        const long uo = long(d.rhs_conf[j]) * d.usz;  // this unit's link offset
         double a0 = 0.0, a1 = 0.0;
         for (int i = beg + threadIdx.x; i < end; i += blockDim.x)
         {
-            const double2 v = f(j, i);
+            const double2 v = f(j, i, uo);
             a0 += v.x;
             a1 += v.y;
         }
@@ -145,14 +152,7 @@ __device__ __forceinline__ Spinor<R> op_site(const SolveDesc& d, bool dag,
                : dirac_site<false, R>(in, U, d.L, s, t, x);
 }
 
-__device__ __forceinline__ const double2* links64(const SolveDesc& d, int j)
-{
-    return d.U64 + long(d.rhs_conf[j]) * d.usz;
-}
-__device__ __forceinline__ const float2* links32(const SolveDesc& d, int j)
-{
-    return d.U32 + long(d.rhs_conf[j]) * d.usz;
-}
+
 
 __device__ __forceinline__ Spinor<float> to32(const Spinor<double>& v)
 {
@@ -171,6 +171,32 @@ __device__ __forceinline__ Spinor<float> axpy(float a, const Spinor<float>& x,
                                               const Spinor<float>& y)
 {
     return {a * x.s0 + y.s0, a * x.s1 + y.s1};
+}
+
+// r + beta p_old formed on the fly: the fused direction update.
+template <typename R>
+struct DirLd
+{
+    const cplx<R>* __restrict__ r;
+    const cplx<R>* __restrict__ p;
+    R beta;
+    __device__ __forceinline__ Spinor<R> sp(long site) const
+    {
+        const Spinor<R> a = ld_spinor(r, site);
+        const Spinor<R> b = ld_spinor(p, site);
+        return {a.s0 + beta * b.s0, a.s1 + beta * b.s1};
+    }
+    __device__ __forceinline__ cplx<R> c(long idx) const { return r[idx] + beta * p[idx]; }
+};
+
+template <typename R, typename Ld>
+__device__ __forceinline__ Spinor<R> op_site_ld(const SolveDesc& d, bool dag, const Ld& in,
+                                                const cplx<R>* __restrict__ U, int i)
+{
+    int s, t, x;
+    site_coords(d.L, i, s, t, x);
+    return dag ? dirac_site_ld<true, R>(in, U, d.L, s, t, x)
+               : dirac_site_ld<false, R>(in, U, d.L, s, t, x);
 }
 
 __device__ void write_outputs(const SolveDesc& d, const Smem& s)
@@ -194,21 +220,21 @@ __device__ bool init_residual(const SolveDesc& d, const Smem& s, int nact, bool 
     const bool dag1 = d.dag_first != 0;
     if (d.has_guess)
     {
-        sweep(d, s.act, nact, s.scratch, false, [&](int j, int i) {
-            const Spinor<double> v = op_site<double>(d, dag1, d.x + j * fs, links64(d, j), i);
+        sweep(d, s.act, nact, s.scratch, false, [&](int j, int i, long uo) {
+            const Spinor<double> v = op_site<double>(d, dag1, d.x + j * fs, d.U64 + uo, i);
             st_spinor(d.t + j * fs, i, v);
             return make_double2(0.0, 0.0);
         });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return false;
     }
-    sweep(d, s.act, nact, s.scratch, true, [&](int j, int i) {
+    sweep(d, s.act, nact, s.scratch, true, [&](int j, int i, long uo) {
         const Spinor<double> b = ld_spinor(d.b + j * fs, i);
         Spinor<double> r = b;
         if (d.has_guess)
         {
             const Spinor<double> a =
-                op_site<double>(d, !dag1, d.t + j * fs, links64(d, j), i);
+                op_site<double>(d, !dag1, d.t + j * fs, d.U64 + uo, i);
             r = {b.s0 - a.s0, b.s1 - a.s1};
         }
         st_spinor(d.r + j * fs, i, r);
@@ -242,7 +268,8 @@ __device__ bool converged_now(const SolveDesc& d, double rr, double bb)
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) cg64_kernel(SolveDesc d)
+template <bool FUSED, int MINB>
+__global__ void __launch_bounds__(256, MINB) cg64_kernel(SolveDesc d)
 {
     const Smem s = carve(d.nrhs);
     for (int j = threadIdx.x; j < d.nrhs; j += blockDim.x)
@@ -270,9 +297,20 @@ __global__ void __launch_bounds__(256) cg64_kernel(SolveDesc d)
 
     for (int it = 1; it <= d.maxiter && nact > 0; ++it)
     {
-        // phase 1: t = D1 p, <p, A p> = |t|^2
-        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i) {
-            const Spinor<double> v = op_site<double>(d, dag1, d.p + j * fs, links64(d, j), i);
+        double2* pc = (FUSED && !(it & 1)) ? d.p2 : d.p;  // direction of this iteration
+        const double2* po = (pc == d.p) ? d.p2 : d.p;     // previous direction
+        const bool fuse = FUSED && it > 1;
+        // phase 1: p = r + beta p_old, t = D1 p, <p, A p> = |t|^2
+        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i, long uo) {
+            Spinor<double> v;
+            if (!fuse)
+                v = op_site<double>(d, dag1, pc + j * fs, d.U64 + uo, i);
+            else
+            {
+                const DirLd<double> ld{d.r + j * fs, po + j * fs, s.cf[j]};
+                v = op_site_ld<double>(d, dag1, ld, d.U64 + uo, i);
+                st_spinor(pc + j * fs, i, ld.sp(i));
+            }
             st_spinor(d.t + j * fs, i, v);
             return make_double2(spinor_norm2(v), 0.0);
         });
@@ -288,16 +326,16 @@ __global__ void __launch_bounds__(256) cg64_kernel(SolveDesc d)
                 s.iters[j] = it;
             }
             else
-                s.cf[j] = s.rr[j] / s.aux[j];
+                s.al[j] = s.rr[j] / s.aux[j];
         }
         __syncthreads();
         nact = compact(d.nrhs, s.act, s.scratch, [&](int j) { return s.state[j] == RHS_ACTIVE; });
 
         // phase 2: x += alpha p; r -= alpha A p
-        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i) {
-            const double a = s.cf[j];
-            const Spinor<double> ap = op_site<double>(d, !dag1, d.t + j * fs, links64(d, j), i);
-            const Spinor<double> p = ld_spinor(d.p + j * fs, i);
+        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i, long uo) {
+            const double a = s.al[j];
+            const Spinor<double> ap = op_site<double>(d, !dag1, d.t + j * fs, d.U64 + uo, i);
+            const Spinor<double> p = ld_spinor(pc + j * fs, i);
             const Spinor<double> x = ld_spinor(d.x + j * fs, i);
             const Spinor<double> r = ld_spinor(d.r + j * fs, i);
             st_spinor(d.x + j * fs, i, axpy(a, p, x));
@@ -327,11 +365,12 @@ __global__ void __launch_bounds__(256) cg64_kernel(SolveDesc d)
         }
         __syncthreads();
         nact = compact(d.nrhs, s.act, s.scratch, [&](int j) { return s.state[j] == RHS_ACTIVE; });
+        if (FUSED)
+            continue;
         if (nact == 0)
             break;
-
         // phase 3: p = r + beta p
-        sweep(d, s.act, nact, s.scratch, false, [&](int j, int i) {
+        sweep(d, s.act, nact, s.scratch, false, [&](int j, int i, long uo) {
             const Spinor<double> p = ld_spinor(d.p + j * fs, i);
             const Spinor<double> r = ld_spinor(d.r + j * fs, i);
             st_spinor(d.p + j * fs, i, axpy(s.cf[j], p, r));
@@ -348,7 +387,8 @@ __global__ void __launch_bounds__(256) cg64_kernel(SolveDesc d)
 // replaces the residual by the FP64 true residual b - A x whenever the FP32
 // residual has dropped by `delta` since the last update, or when it claims
 // convergence. A right-hand side converges only on the FP64 true residual.
-__global__ void __launch_bounds__(256) cg_mixed_kernel(SolveDesc d)
+template <bool FUSED, int MINB>
+__global__ void __launch_bounds__(256, MINB) cg_mixed_kernel(SolveDesc d)
 {
     const Smem s = carve(d.nrhs);
     for (int j = threadIdx.x; j < d.nrhs; j += blockDim.x)
@@ -378,8 +418,19 @@ __global__ void __launch_bounds__(256) cg_mixed_kernel(SolveDesc d)
     // stall counters live in the upper bits of flag: flag = 2*stalls + update bit
     for (int it = 1; it <= d.maxiter && nact > 0; ++it)
     {
-        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i) {
-            const Spinor<float> v = op_site<float>(d, dag1, d.p32 + j * fs, links32(d, j), i);
+        float2* pc = (FUSED && !(it & 1)) ? d.p32b : d.p32;
+        const float2* po = (pc == d.p32) ? d.p32b : d.p32;
+        const bool fuse = FUSED && it > 1;
+        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i, long uo) {
+            Spinor<float> v;
+            if (!fuse)
+                v = op_site<float>(d, dag1, pc + j * fs, d.U32 + uo, i);
+            else
+            {
+                const DirLd<float> ld{d.r32 + j * fs, po + j * fs, float(s.cf[j])};
+                v = op_site_ld<float>(d, dag1, ld, d.U32 + uo, i);
+                st_spinor(pc + j * fs, i, ld.sp(i));
+            }
             st_spinor(d.t32 + j * fs, i, v);
             return make_double2(spinor_norm2(v), 0.0);
         });
@@ -395,15 +446,15 @@ __global__ void __launch_bounds__(256) cg_mixed_kernel(SolveDesc d)
                 s.iters[j] = it;
             }
             else
-                s.cf[j] = s.rr[j] / s.aux[j];
+                s.al[j] = s.rr[j] / s.aux[j];
         }
         __syncthreads();
         nact = compact(d.nrhs, s.act, s.scratch, [&](int j) { return s.state[j] == RHS_ACTIVE; });
 
-        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i) {
-            const float a = float(s.cf[j]);
-            const Spinor<float> ap = op_site<float>(d, !dag1, d.t32 + j * fs, links32(d, j), i);
-            const Spinor<float> p = ld_spinor(d.p32 + j * fs, i);
+        sweep(d, s.act, nact, s.scratch, true, [&](int j, int i, long uo) {
+            const float a = float(s.al[j]);
+            const Spinor<float> ap = op_site<float>(d, !dag1, d.t32 + j * fs, d.U32 + uo, i);
+            const Spinor<float> p = ld_spinor(pc + j * fs, i);
             const Spinor<float> e = ld_spinor(d.e32 + j * fs, i);
             const Spinor<float> r = ld_spinor(d.r32 + j * fs, i);
             st_spinor(d.e32 + j * fs, i, axpy(a, p, e));
@@ -426,21 +477,20 @@ __global__ void __launch_bounds__(256) cg_mixed_kernel(SolveDesc d)
             s.rr[j] = rn;
         }
         __syncthreads();
-        const int nru =
-            compact(d.nrhs, s.act + d.nrhs * 0, s.scratch, [&](int j) {
-                return s.state[j] == RHS_ACTIVE && (s.flag[j] & 1);
-            });
+        const int nru = compact(d.nrhs, s.act, s.scratch, [&](int j) {
+            return s.state[j] == RHS_ACTIVE && (s.flag[j] & 1);
+        });
         if (nru > 0)
         {
             // Reliable update, part 1: t = D1 (x + e) in FP64, with x + e
             // formed on the fly from its neighbourhood and parked in r.
-            sweep(d, s.act, nru, s.scratch, false, [&](int j, int i) {
+            sweep(d, s.act, nru, s.scratch, false, [&](int j, int i, long uo) {
                 int ss, tt, xx;
                 site_coords(d.L, i, ss, tt, xx);
                 const SumLd xe{d.x + j * fs, d.e32 + j * fs};
                 const Spinor<double> v =
-                    dag1 ? dirac_site_ld<true, double>(xe, links64(d, j), d.L, ss, tt, xx)
-                         : dirac_site_ld<false, double>(xe, links64(d, j), d.L, ss, tt, xx);
+                    dag1 ? dirac_site_ld<true, double>(xe, d.U64 + uo, d.L, ss, tt, xx)
+                         : dirac_site_ld<false, double>(xe, d.U64 + uo, d.L, ss, tt, xx);
                 st_spinor(d.t + j * fs, i, v);
                 st_spinor(d.r + j * fs, i, xe.sp(i));
                 return make_double2(0.0, 0.0);
@@ -448,9 +498,9 @@ __global__ void __launch_bounds__(256) cg_mixed_kernel(SolveDesc d)
             if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
                 return;
             // part 2: x = x + e; r = b - D2 t; r32 = r; e = 0
-            sweep(d, s.act, nru, s.scratch, true, [&](int j, int i) {
+            sweep(d, s.act, nru, s.scratch, true, [&](int j, int i, long uo) {
                 const Spinor<double> xn = ld_spinor(d.r + j * fs, i);
-                const Spinor<double> a = op_site<double>(d, !dag1, d.t + j * fs, links64(d, j), i);
+                const Spinor<double> a = op_site<double>(d, !dag1, d.t + j * fs, d.U64 + uo, i);
                 const Spinor<double> b = ld_spinor(d.b + j * fs, i);
                 st_spinor(d.x + j * fs, i, xn);
                 const Spinor<double> r = {b.s0 - a.s0, b.s1 - a.s1};
@@ -482,9 +532,11 @@ __global__ void __launch_bounds__(256) cg_mixed_kernel(SolveDesc d)
             __syncthreads();
         }
         nact = compact(d.nrhs, s.act, s.scratch, [&](int j) { return s.state[j] == RHS_ACTIVE; });
+        if (FUSED)
+            continue;
         if (nact == 0)
             break;
-        sweep(d, s.act, nact, s.scratch, false, [&](int j, int i) {
+        sweep(d, s.act, nact, s.scratch, false, [&](int j, int i, long uo) {
             const Spinor<float> p = ld_spinor(d.p32 + j * fs, i);
             const Spinor<float> r = ld_spinor(d.r32 + j * fs, i);
             st_spinor(d.p32 + j * fs, i, axpy(float(s.cf[j]), p, r));
@@ -495,5 +547,13 @@ __global__ void __launch_bounds__(256) cg_mixed_kernel(SolveDesc d)
     }
     write_outputs(d, s);
 }
+
+// Instances: the fused two-barrier form at two blocks per SM wins when a
+// single right-hand side is latency bound; the three-barrier form at three
+// blocks per SM wins for batches (fewer loads per site).
+template __global__ void cg64_kernel<true, 2>(SolveDesc);
+template __global__ void cg64_kernel<false, 3>(SolveDesc);
+template __global__ void cg_mixed_kernel<true, 2>(SolveDesc);
+template __global__ void cg_mixed_kernel<false, 3>(SolveDesc);
 
 }  // namespace dwfb

@@ -24,10 +24,12 @@ struct SolveDesc
     const double2* b;
     double2* x;
     double2* r;
-    double2* p;
+    double2* p;    // search direction, double-buffered with p2
+    double2* p2;
     double2* t;
     float2* r32;
-    float2* p32;
+    float2* p32;   // FP32 search direction, double-buffered with p32b
+    float2* p32b;
     float2* t32;
     float2* e32;
     double* part;  // partial sums [nrhs][nch][2]
@@ -52,10 +54,12 @@ struct SolveDesc
 // Dynamic shared memory needed by the solver kernels for nrhs right-hand sides.
 inline size_t solver_smem_bytes(int nrhs)
 {
-    return 64 * sizeof(double) + size_t(nrhs) * (5 * sizeof(double) + 5 * sizeof(int));
+    return 64 * sizeof(double) + size_t(nrhs) * (6 * sizeof(double) + 5 * sizeof(int));
 }
 
+template <bool FUSED, int MINB>
 __global__ void cg64_kernel(SolveDesc d);
+template <bool FUSED, int MINB>
 __global__ void cg_mixed_kernel(SolveDesc d);
 
 }  // namespace dwfb

@@ -66,6 +66,39 @@ int ensure_workspace(dwf_ctx* c, int nrhs)
     return DWF_OK;
 }
 
+void choose_units(int nsite, int nrhs, long cap, int* nch_out, int* ch_out, int* grid_out)
+{
+    // Work units = (right-hand side, chunk). Pick the chunk count that fills
+    // the resident blocks in whole waves (every block gets the same number of
+    // units, up to one), preferring fewer, larger chunks.
+    int best_nch = 1;
+    long best_waves = 1;
+    double best_eff = -1.0;
+    for (int nch = 1; nch <= 4096; ++nch)
+    {
+        const long ch_try = (nsite + nch - 1) / nch;
+        if (nch > 1 && ch_try < 128)
+            break;
+        const long u = long(nrhs) * nch;
+        const long waves = (u + cap - 1) / cap;
+        const double eff = double(u) / double(waves * cap);
+        if (eff > best_eff + 0.02)
+        {
+            best_eff = eff;
+            best_nch = nch;
+            best_waves = waves;
+        }
+        if (eff >= 0.95)
+            break;
+    }
+    const int ch = (nsite + best_nch - 1) / best_nch;
+    const int nch = (nsite + ch - 1) / ch;
+    const long units = long(nrhs) * nch;
+    *nch_out = nch;
+    *ch_out = ch;
+    *grid_out = int(std::min<long>(cap, (units + best_waves - 1) / best_waves));
+}
+
 int ensure_part(dwf_ctx* c, size_t n)
 {
     if (n <= c->w_part_cap)
@@ -221,37 +254,14 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     if (bps < 1)
         return ctx_fail(c, DWF_CUDA_ERROR, "solver kernel cannot be resident");
     const int cap = bps * c->nsm;
-    // Work units = (right-hand side, chunk). Pick the chunk count that fills
-    // the resident blocks in whole waves (every block gets the same number of
-    // units, up to one), preferring fewer, larger chunks.
-    const int nsite = c->L.nsite;
-    int best_nch = 1, best_waves = 1;
-    double best_eff = -1.0;
-    for (int nch = 1; nch <= 4096; ++nch)
-    {
-        const long ch_try = (nsite + nch - 1) / nch;
-        if (nch > 1 && ch_try < kSolverThreads / 2)
-            break;
-        const long u = long(nrhs) * nch;
-        const long waves = (u + cap - 1) / cap;
-        const double eff = double(u) / double(waves * cap);
-        if (eff > best_eff + 0.02)
-        {
-            best_eff = eff;
-            best_nch = nch;
-            best_waves = int(waves);
-        }
-        if (eff >= 0.95)
-            break;
-    }
-    d.nch = best_nch;
-    d.ch = (nsite + best_nch - 1) / best_nch;
+    int grid_blocks = 0;
+    choose_units(c->L.nsite, nrhs, cap, &d.nch, &d.ch, &grid_blocks);
     const long units = long(nrhs) * d.nch;
     int st = ensure_part(c, size_t(units) * 2);
     if (st)
         return st;
     d.part = c->w_part;
-    const int grid = int(std::min<long>(cap, (units + best_waves - 1) / best_waves));
+    const int grid = grid_blocks;
     d.expected_blocks = unsigned(grid);
     CK(cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->stream));
     void* args[] = {&d};

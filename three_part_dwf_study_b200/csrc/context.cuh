@@ -78,6 +78,9 @@ namespace dwfb {
 int ctx_fail(dwf_ctx* c, int code, const std::string& msg);
 int ensure_workspace(dwf_ctx* c, int nrhs);
 int ensure_part(dwf_ctx* c, size_t n);
+// Chunks per right-hand side, sites per chunk and grid size of a persistent
+// solver launch over nrhs right-hand sides with `cap` resident blocks.
+void choose_units(int nsite, int nrhs, long cap, int* nch, int* ch, int* grid);
 // Batched solve on device fields (b, x: nrhs fields of fsz complex doubles).
 int solve_batch(dwf_ctx* c, int op, int nrhs, const int* conf_h, const double2* b, double2* x,
                 int has_guess, double rtol, int maxiter, int solver, int eigen_rule,

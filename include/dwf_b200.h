@@ -287,6 +287,29 @@ int dwf_rng_pseudofermion(dwf_rng* rng, long n, double* chi);
 /* n Z4 digits from mt19937_64(seed) (correlator.hpp:35-58). */
 int dwf_z4_digits(uint64_t seed, long n, signed char* out);
 
+/* ---- allocation-free solve ------------------------------------------------------ */
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory (code recording a CUDA graph on another thread, plugins confined to
+ * their host application's memory pool, allocator-free latency loops):
+ * the reference FP64 CG (as DWF_SOLVER_CG64) for one domain-wall right-hand
+ * side, needing no context and calling no cudaMalloc, cudaFree or allocating
+ * library routine. The caller passes device pointers it owns: theta_dev
+ * (2*Nt*Nx angles), b_dev and x_dev (Ls*Nt*Nx*2 complex<double>; x read as the
+ * guess when has_guess), and a cudaStream_t (or NULL) as void*. All other
+ * buffers live in one static device array that each GPU loading the library
+ * holds until exit: lattices up to DWF_NOALLOC_MAX_SITES = Ls*Nt*Nx sites and
+ * DWF_NOALLOC_MAX_LINKS = 2*Nt*Nx links; larger ones return DWF_BAD_ARG.
+ * params->device selects (and leaves current) the GPU. The first call on a
+ * device resolves the array's device address, so make that first call before
+ * any stream capture. Calls share the array: calls whose GPU work overlaps
+ * race and must be serialised by the caller. Returns the solve status; info
+ * (host, may be NULL) as dwf_cg reports it. */
+#define DWF_NOALLOC_MAX_SITES 65536
+#define DWF_NOALLOC_MAX_LINKS 32768
+int dwf_cg_noalloc(const dwf_params* params, int op, const double* theta_dev, const void* b_dev,
+                   void* x_dev, int has_guess, double rtol, int maxiter, void* stream,
+                   dwf_solve_info* info);
+
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);
 /* Accumulated device time (ms) of the persistent solver launches, measured

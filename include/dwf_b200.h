@@ -243,7 +243,7 @@ typedef struct
     int n_point_times;
     int n_wall_times;
     int n_noise;      /* eta.noise_vectors */
-    int max_momentum; /* analysis.max_momentum (0..Nx/2, at most 15) */
+    int max_momentum; /* analysis.max_momentum (0..Nx/2) */
     double rtol;      /* dwf.propagator_rtol */
     int maxiter;      /* dwf.propagator_maxiter */
     int solver;       /* dwf_solver */
@@ -309,6 +309,12 @@ int dwf_z4_digits(uint64_t seed, long n, signed char* out);
 int dwf_cg_noalloc(const dwf_params* params, int op, const double* theta_dev, const void* b_dev,
                    void* x_dev, int has_guess, double rtol, int maxiter, void* stream,
                    dwf_solve_info* info);
+
+/* Self test of the bounded grid barrier used by every persistent kernel: one
+ * block per SM passes 8 barriers that expect missing_blocks more arrivals than
+ * there are blocks. missing_blocks = 0 returns DWF_OK; > 0 makes every wait run
+ * into limit_ns and returns DWF_TIMEOUT with the context still usable. */
+int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
 
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);

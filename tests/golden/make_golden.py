@@ -59,6 +59,10 @@ CASES = {
     "wil_6x10": ("wil", {"wilson.Nt": 6, "wilson.Nx": 10, "wilson.m0": 0.3,
                          "wilson.source_t": 2, "wilson.source_x": 3,
                          "wilson.space_boundary_sign": -1.0}, 22),
+    "wil_hmc_8x8": ("wil_hmc", {"wilson.trajectories": 6, "wilson.m0": 0.3,
+                                "wilson.trajectory_length": 0.5, "wilson.hmc_steps": 5,
+                                "analysis.plateau_window_size": 2,
+                                "analysis.plateau_flatness_tolerance": 10.0}, None),
 }
 
 
@@ -115,6 +119,13 @@ def main():
                           "correlator.csv", "channels_by_config.csv",
                           "momentum_correlators.csv"]:
                     shutil.copy2(tmp / "output" / "domain_wall" / f, dest / f)
+            elif kind == "wil_hmc":
+                (tmp / "output" / "wilson").mkdir(parents=True)
+                run([str(REF_BIN / "generate_wilson")], tmp)
+                run([str(REF_BIN / "analyze_wilson")], tmp)
+                for f in ["wilson_ensemble.bin", "hmc_history.csv",
+                          "correlators_by_config.csv"]:
+                    shutil.copy2(tmp / "output" / "wilson" / f, dest / f)
             for f in sorted(tmp.glob("*.npy")):
                 shutil.copy2(f, dest / f.name)
             shutil.copy2(tmp / "parameters.txt", dest / "parameters.txt")

@@ -178,3 +178,22 @@ def test_batched_solve_many_configs(tdwf):
             if solver == tdwf.SOLVER_CG64:
                 x1, it1, _, _ = o.cg(3, ths[conf[k]], bs[k], 1e-11, 4000)
                 assert abs(infos[k]["iterations"] - it1) <= 2
+
+
+def test_bounded_barrier_times_out_and_context_survives(tdwf):
+    """A grid barrier that can never complete (more arrivals expected than
+    blocks exist) ends in DWF_TIMEOUT after its limit; the same context then
+    solves normally."""
+    import time
+    from three_part_dwf_study_b200 import _capi as A
+    d = tdwf.DomainWall(8, 8, 4, 1.0, 0.1)
+    assert A.lib().dwf_barrier_selftest(d.handle, 0, 1_000_000_000) == A.DWF_OK
+    t0 = time.perf_counter()
+    assert A.lib().dwf_barrier_selftest(d.handle, 1, 50_000_000) == A.DWF_TIMEOUT
+    assert time.perf_counter() - t0 < 5.0
+    assert "ran out" in A.lib().dwf_last_error(d.handle).decode()
+    rng = np.random.default_rng(5)
+    th = random_theta(rng, 8, 8)
+    b = random_field(rng, d.Ndof)
+    r = d.conjugate_gradient(3, th, b, rtol=1e-10, maxiter=2000)
+    assert r.converged and r.info["true_relres"] < 1e-9

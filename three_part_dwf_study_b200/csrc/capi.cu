@@ -713,6 +713,29 @@ int dwf_propagators(dwf_ctx* c, int nrhs, const int* rhs_conf, const double* src
 
 uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
 
+int dwf_barrier_selftest(dwf_ctx* c, int missing_blocks, uint64_t limit_ns)
+{
+    if (!c || missing_blocks < 0 || limit_ns == 0)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    const unsigned grid = unsigned(std::max(1, c->nsm));
+    CK(cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->stream));
+    const unsigned expected = grid + unsigned(missing_blocks);
+    unsigned long long lim = limit_ns;
+    int rounds = 8;
+    GridBar* bar = c->bar;
+    void* args[] = {&bar, const_cast<unsigned*>(&expected), &lim, &rounds};
+    CK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&barrier_probe_kernel), dim3(grid),
+                                   dim3(32), args, 0, c->stream));
+    c->launches += 1;
+    GridBar hb{};
+    CK(cudaMemcpyAsync(&hb, c->bar, sizeof(GridBar), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (hb.err != 0)
+        return ctx_fail(c, hb.err, "grid barrier wait ran out");
+    return DWF_OK;
+}
+
 double dwf_solver_kernel_ms(const dwf_ctx* c, uint64_t* nlaunch)
 {
     if (!c)

@@ -102,4 +102,15 @@ __global__ void residual_finish_kernel(const double* __restrict__ part, int nrhs
         out[j] = bb > 0.0 ? sqrt(rr / bb) : 0.0;
 }
 
+// Every block passes `rounds` grid barriers that expect `expected` arrivals.
+// With expected > gridDim.x no barrier can complete: each wait runs into its
+// limit and records DWF_TIMEOUT, and every block returns.
+__global__ void barrier_probe_kernel(GridBar* bar, unsigned expected, unsigned long long timeout_ns,
+                                     int rounds)
+{
+    for (int k = 0; k < rounds; ++k)
+        if (!grid_sync(bar, expected, timeout_ns))
+            return;
+}
+
 }  // namespace dwfb

@@ -28,4 +28,8 @@ __global__ void residual_partials_kernel(Lat L, const double2* __restrict__ t,
 __global__ void residual_finish_kernel(const double* __restrict__ part, int nrhs, int nch,
                                        double* __restrict__ out);
 
+// Grid-barrier self test (see dwf_barrier_selftest).
+__global__ void barrier_probe_kernel(GridBar* bar, unsigned expected, unsigned long long timeout_ns,
+                                     int rounds);
+
 }  // namespace dwfb

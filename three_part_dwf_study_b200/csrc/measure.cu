@@ -95,41 +95,51 @@ __global__ void sources_kernel(SrcDesc d, long nrhs, double2* __restrict__ src)
 //   [0] |q|^2, [1] Re(psi(Ls/2)^dag q), [2+n] cos(2 pi n x / Nx) |q|^2,
 // with q = P_L psi(s=0) + P_R psi(s=Ls-1) = (psi_0(Ls-1), psi_1(0))
 // (correlator.hpp:149-174, :258-301). Wilson (ls_src = 0): [0] = sum_x sum_a
-// |psi_a(t,x)|^2 (wilson/include/correlator.hpp:32-39).
+// |psi_a(t,x)|^2 (wilson/include/correlator.hpp:32-39). The per-x values are
+// staged in shared memory (2*Nx doubles); each output is one warp's fixed-order
+// sum over x.
 __global__ void contract_kernel(Lat L, int ls_src, int nmom, const double2* __restrict__ psi,
                                 double* __restrict__ red)
 {
-    __shared__ double scratch[64];
+    extern __shared__ double sx[];  // [Nx] |q|^2, [Nx] J5
     const long j = blockIdx.y;
     const int t = blockIdx.x;
     const int K = 2 + nmom;
     const double2* P = psi + j * 2L * L.nsite;
-    double acc[2 + 16];
-    for (int k = 0; k < K; ++k)
-        acc[k] = 0.0;
+    double* qq = sx;
+    double* j5 = sx + L.Nx;
     for (int x = threadIdx.x; x < L.Nx; x += blockDim.x)
     {
         const int site = t * L.Nx + x;
         if (!ls_src)
         {
-            const Spinor<double> v = ld_spinor(P, site);
-            acc[0] += spinor_norm2(v);
+            qq[x] = spinor_norm2(ld_spinor(P, site));
+            j5[x] = 0.0;
             continue;
         }
         const double2 q0 = P[2 * (long(L.Ls - 1) * L.V + site)];
-        const double2 q1 = P[2 * (long(0) * L.V + site) + 1];
+        const double2 q1 = P[2 * long(site) + 1];
         const Spinor<double> mid = ld_spinor(P, long(L.Ls / 2) * L.V + site);
-        const double qq = norm2(q0) + norm2(q1);
-        acc[0] += qq;
-        acc[1] += mid.s0.x * q0.x + mid.s0.y * q0.y + mid.s1.x * q1.x + mid.s1.y * q1.y;
-        for (int n = 0; n < nmom; ++n)
-            acc[2 + n] += cos(2.0 * 3.141592653589793238462643383279502884 * n / L.Nx * x) * qq;
+        qq[x] = norm2(q0) + norm2(q1);
+        j5[x] = mid.s0.x * q0.x + mid.s0.y * q0.y + mid.s1.x * q1.x + mid.s1.y * q1.y;
     }
-    for (int k = 0; k < K; ++k)
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = w; k < K; k += nw)
     {
-        const double v = block_sum(acc[k], scratch);
-        if (threadIdx.x == 0)
-            red[(j * L.Nt + t) * K + k] = v;
+        double acc = 0.0;
+        for (int x = lane; x < L.Nx; x += 32)
+        {
+            if (k == 0)
+                acc += qq[x];
+            else if (k == 1)
+                acc += j5[x];
+            else
+                acc += cos(2.0 * 3.141592653589793238462643383279502884 * (k - 2) / L.Nx * x) * qq[x];
+        }
+        acc = warp_sum(acc);
+        if (lane == 0)
+            red[(j * L.Nt + t) * K + k] = acc;
     }
 }
 
@@ -199,7 +209,7 @@ int dwf_measure(dwf_ctx* c, const dwf_measure_params* mp, int nconf, const doubl
     if (!c || !mp || !thetas || nconf < 1 || c->kind != 0)
         return DWF_BAD_ARG;
     if (mp->n_point_times < 0 || mp->n_wall_times < 0 || mp->n_noise < 0 ||
-        mp->max_momentum < 0 || mp->max_momentum > c->L.Nx / 2 || mp->max_momentum > 15)
+        mp->max_momentum < 0 || mp->max_momentum > c->L.Nx / 2)
         return ctx_fail(c, DWF_BAD_ARG, "analysis.max_momentum is outside 0..Nx/2");
     if (mp->n_noise > 0 && !z4)
         return ctx_fail(c, DWF_BAD_ARG, "measure: z4 digits required for noise sources");
@@ -251,8 +261,8 @@ int dwf_measure(dwf_ctx* c, const dwf_measure_params* mp, int nconf, const doubl
     for (long j = 0; j < nrhs; j += 65535)
     {
         const int n = int(std::min<long>(65535, nrhs - j));
-        contract_kernel<<<dim3(c->L.Nt, n), 128, 0, c->stream>>>(c->L, 1, nmom, B.x + j * fs,
-                                                                 B.red + j * c->L.Nt * K);
+        contract_kernel<<<dim3(c->L.Nt, n), 128, 2 * c->L.Nx * sizeof(double), c->stream>>>(
+            c->L, 1, nmom, B.x + j * fs, B.red + j * c->L.Nt * K);
         c->launches += 1;
     }
     if (mp->n_noise > 0)
@@ -391,8 +401,8 @@ int wil_pseudoscalar_correlator(dwf_ctx* c, int nconf, const double* thetas, int
     for (long j = 0; j < nrhs; j += 65535)
     {
         const int n = int(std::min<long>(65535, nrhs - j));
-        contract_kernel<<<dim3(c->L.Nt, n), 128, 0, c->stream>>>(c->L, 0, 0, B.x + j * fs,
-                                                                 B.red + j * c->L.Nt * 2);
+        contract_kernel<<<dim3(c->L.Nt, n), 128, 2 * c->L.Nx * sizeof(double), c->stream>>>(
+            c->L, 0, 0, B.x + j * fs, B.red + j * c->L.Nt * 2);
         c->launches += 1;
     }
     std::vector<double> red(nrhs * c->L.Nt * 2);

@@ -1,0 +1,44 @@
+// Shared helpers of the drop-in headers: status-to-exception mapping and the
+// solver path (DWF_B200_SOLVER=cg64 selects the reference FP64 CG, anything
+// else the mixed FP32/FP64 reliable-update CG; both meet the same rtol).
+#pragma once
+
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "dwf_b200.h"
+
+namespace b200 {
+
+inline int solver()
+{
+    static const int s = [] {
+        const char* v = std::getenv("DWF_B200_SOLVER");
+        return (v && std::strcmp(v, "cg64") == 0) ? DWF_SOLVER_CG64 : DWF_SOLVER_MIXED;
+    }();
+    return s;
+}
+
+inline void check(dwf_ctx* c, int st)
+{
+    if (st == DWF_OK)
+        return;
+    const char* m = c ? dwf_last_error(c) : "";
+    throw std::runtime_error(m && *m ? std::string(m) : std::string(dwf_status_string(st)));
+}
+
+template <typename V>
+inline const double* cptr(const V& v)
+{
+    return reinterpret_cast<const double*>(v.data());
+}
+template <typename V>
+inline double* mptr(V& v)
+{
+    return reinterpret_cast<double*>(v.data());
+}
+
+}  // namespace b200

@@ -123,6 +123,20 @@ def reliable_update_bytes(V, Ls):
     return 2 * dslash_bytes(V, Ls, 8) + V * Ls * (32 + 16 + 32 + 32 + 32 + 16 + 16)
 
 
+def eo_iter_bytes(V, Ls):
+    """One FP32 iteration of the even-odd Schur CG: 17 half-lattice spinor
+    streams of 16 B per site (P1 2, P2 3, P3 2, P4 7, P5 3) and the FP32 links
+    (2V x 8 B) once in each of the four operator phases."""
+    return 17 * (V // 2) * Ls * 16 + 4 * 2 * V * 8
+
+
+def eo_reliable_update_bytes(V, Ls):
+    """FP64 residual replacement of the Schur normal equation: 16 half-lattice
+    FP64-equivalent streams (x, e, y, t, b, parked x+e, r, r32, e32) and the
+    FP64 links in four operator phases."""
+    return 16 * (V // 2) * Ls * 32 + 4 * 2 * V * 16
+
+
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
@@ -333,12 +347,12 @@ def impl_ours(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def timed(fn, steps, warmup, tag):
+    def timed(fn, steps, warmup, kind):
         for _ in range(warmup):
             fn()
         barrier()
         total = 0.0
-        k0, n0 = d.solver_kernel_ms()
+        k0, n0 = d.solver_kernel_ms(kind)
         l0 = d.launch_count()
         infos_all = []
         for _ in range(steps):
@@ -352,8 +366,12 @@ def impl_ours(args):
             e1.synchronize()
             total += e0.elapsed_time(e1) * 1e-3
         barrier()
-        k1, n1 = d.solver_kernel_ms()
+        k1, n1 = d.solver_kernel_ms(kind)
         return total, infos_all, (k1 - k0) * 1e-3, n1 - n0, d.launch_count() - l0
+
+    def step_eo():
+        return d.propagators_dev(src_dev, x_dev, rtol=RTOL, maxiter=MAXITER,
+                                 solver=T.SOLVER_EO_MIXED)
 
     def step_mixed():
         return d.propagators_dev(src_dev, x_dev, rtol=RTOL, maxiter=MAXITER,
@@ -364,12 +382,13 @@ def impl_ours(args):
                                  solver=T.SOLVER_CG64)
 
     with ClockSampler(local) as clk:
-        t_mixed, infos_m, kern_s, nkern, launches = timed(step_mixed, args.steps, args.warmup,
-                                                          "mixed")
+        t_mixed, infos_m, kern_s, nkern, launches = timed(step_eo, args.steps, args.warmup, 1)
     clocks = clk.summary()
-    t_fp64, infos_f, kern64_s, nkern64, _ = timed(step_fp64, max(1, args.steps // 2), 1, "fp64")
+    n_side = max(1, args.steps // 2)
+    t_fp64, infos_f, kern64_s, nkern64, _ = timed(step_fp64, n_side, 1, 0)
+    t_full, infos_full, _, _, _ = timed(step_mixed, n_side, 1, 0)
 
-    for infos in infos_m + infos_f:
+    for infos in infos_m + infos_f + infos_full:
         for i in infos:
             if not i["converged"] or i["true_relres"] > RTOL * 1.0001:
                 raise SystemExit(f"solve did not reach the FP64 true residual: {i}")
@@ -386,7 +405,8 @@ def impl_ours(args):
     t_mixed_max = allmax(t_mixed)
     t_fp64_max = allmax(t_fp64)
     value = ws * nrhs * args.steps / t_mixed_max
-    fp64_value = ws * nrhs * max(1, args.steps // 2) / t_fp64_max
+    fp64_value = ws * nrhs * n_side / t_fp64_max
+    full_value = ws * nrhs * n_side / allmax(t_full)
 
     # ---- end to end through the host C ABI ----
     src_host = torch.from_numpy(srcs.view(np.float64).copy()).pin_memory()
@@ -404,7 +424,7 @@ def impl_ours(args):
         infos = (A.SolveInfo * nrhs)()
         A.check(A.lib().dwf_propagators(d.handle, nrhs, None, C.c_void_p(src_np.ctypes.data),
                                         C.c_void_p(x_np.ctypes.data), RTOL, MAXITER,
-                                        T.SOLVER_MIXED, infos), d.handle)
+                                        T.SOLVER_EO_MIXED, infos), d.handle)
         return infos
 
     for _ in range(args.warmup):
@@ -454,20 +474,20 @@ def impl_ours(args):
     dslash["lattice"] = list(DSLASH_LATTICE)
     dslash["bytes_rule"] = "V*(Ls*64+32) B (FP64), V*(Ls*32+16) B (FP32) per application"
 
-    # ---- roofline of the dominant kernel (the persistent mixed solver) ----
+    # ---- roofline of the dominant kernel (the persistent even-odd solver) ----
     V = NT * NX
-    iters = sum(i["iterations"] for infos in infos_m for i in infos)
+    iters = sum(i["schur_iterations"] for infos in infos_m for i in infos)
     rus = sum(i["reliable_updates"] for infos in infos_m for i in infos)
-    alg_bytes = iters * cg_iter_bytes(V, LS, 4) + rus * reliable_update_bytes(V, LS)
+    alg_bytes = iters * eo_iter_bytes(V, LS) + rus * eo_reliable_update_bytes(V, LS)
     kernel_launch_s = kern_s / max(1, nkern)
     achieved = alg_bytes / max(1, nkern) / kernel_launch_s / 1e9
     traffic = None
     tfile = REPO / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("cg_mixed_kernel_bytes_per_launch")
+        traffic = json.loads(tfile.read_text()).get("cg_eo_mixed_kernel_bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "cg_mixed_kernel", "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+                "kernel": "cg_eo_mixed_kernel", "peak_kind": f"{peak_kind} hbm_gbs (burst)",
                 "alg_bytes_per_launch": alg_bytes / max(1, nkern),
                 "kernel_ms_per_launch": kernel_launch_s * 1e3,
                 "kernel_share_of_step": kern_s / t_mixed}
@@ -479,13 +499,19 @@ def impl_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64 (FP32 inner CG, FP64 reliable updates and true residual)",
         "data": "synthetic (seeded hot-start links, boundary point/Z4/wall sources)",
-        "config": dict(workload_config("mixed FP32/FP64 reliable-update CG"),
+        "config": dict(workload_config("even-odd Schur mixed FP32/FP64 CG, then the full "
+                                       "D^dag D check"),
                        parallelism=f"dp{ws} (independent configurations per rank)"),
         "plain_fp64_cg": {"value": fp64_value, "unit": "solves/s",
                           "speedup_of_value": value / fp64_value,
                           "iterations_mean": statistics.mean(
                               i["iterations"] for infos in infos_f for i in infos)},
+        "mixed_full_lattice_cg": {"value": full_value, "unit": "solves/s",
+                                  "iterations_mean": statistics.mean(
+                                      i["iterations"] for infos in infos_full for i in infos)},
         "iterations_mean": statistics.mean(i["iterations"] for infos in infos_m for i in infos),
+        "schur_iterations_mean": statistics.mean(
+            i["schur_iterations"] for infos in infos_m for i in infos),
         "e2e": {"value": e2e_value, "unit": "solves/s",
                 "h2d_bytes_per_step": int(src_np.nbytes + th_np.nbytes),
                 "d2h_bytes_per_step": int(x_np.nbytes),
@@ -530,14 +556,15 @@ def calibrate_reference():
 
 
 def profile_case():
-    """One mixed and one FP64 propagator batch of the workload (for ncu)."""
+    """One even-odd, one full-lattice mixed and one FP64 propagator batch of the
+    workload (for ncu)."""
     import torch
     import three_part_dwf_study_b200 as T
     d = T.DomainWall(NT, NX, LS, M5, MF, BETA)
     d.set_gauge(workload_gauge(0))
     src = torch.from_numpy(workload_sources(0).view(np.float64).copy()).cuda()
     x = torch.zeros_like(src)
-    for solver in (T.SOLVER_MIXED, T.SOLVER_CG64):
+    for solver in (T.SOLVER_EO_MIXED, T.SOLVER_MIXED, T.SOLVER_CG64):
         infos = d.propagators_dev(src, x, rtol=RTOL, maxiter=MAXITER, solver=solver)
         assert all(i["converged"] for i in infos)
     d.close()

@@ -66,7 +66,14 @@ typedef enum
      * recomputed in FP64); converged only when the FP64 true residual meets
      * rtol. Falls back to DWF_SOLVER_CG64 from its current iterate if the
      * true residual stalls. */
-    DWF_SOLVER_MIXED = 1
+    DWF_SOLVER_MIXED = 1,
+    /* Propagator solves (dwf_propagators, dwf_measure): even-odd
+     * (4-D checkerboard) Schur-complement preconditioned mixed CG for
+     * D x = src, then DWF_SOLVER_MIXED on the full D^dag D from that x, so the
+     * reference's stopping rule on the full normal equation decides. Needs even
+     * Nt, Nx and 3 - M5 >= 1 (else it runs DWF_SOLVER_MIXED); elsewhere it is
+     * DWF_SOLVER_MIXED. */
+    DWF_SOLVER_EO_MIXED = 2
 } dwf_solver;
 
 /* Domain-wall context parameters: the parameters.txt keys dwf.Nt, dwf.Nx,
@@ -91,6 +98,8 @@ typedef struct
     int reliable_updates;/* FP64 residual replacements (mixed path) */
     int fallback;        /* 1 if the mixed path fell back to FP64 CG */
     double dirac_relres; /* propagator solves: |D x - src| / |src| (correlator.hpp:225-227); else 0 */
+    int schur_iterations;/* DWF_SOLVER_EO_MIXED: iterations of the even-odd stage (included
+                            in `iterations`); else 0 */
 } dwf_solve_info;
 
 typedef struct dwf_ctx dwf_ctx;
@@ -318,9 +327,10 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
 
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);
-/* Accumulated device time (ms) of the persistent solver launches, measured
- * with CUDA events on the context stream; *nlaunch (optional) = their count. */
-double dwf_solver_kernel_ms(const dwf_ctx* ctx, uint64_t* nlaunch);
+/* Accumulated device time (ms) of the persistent solver launches of one kind
+ * (0: full-lattice CG kernels, 1: the even-odd Schur kernel), measured with
+ * CUDA events on the context stream; *nlaunch (optional) = their count. */
+double dwf_solver_kernel_ms(const dwf_ctx* ctx, int kind, uint64_t* nlaunch);
 
 #ifdef __cplusplus
 }

@@ -14,7 +14,7 @@ LIB_PATH = Path(os.environ.get("DWF_B200_LIB", _PKG / "_lib" / "libdwfb200.so"))
 DWF_OK, DWF_NOT_CONVERGED, DWF_ZERO_DENOM, DWF_NONFINITE = 0, 1, 2, 3
 DWF_CUDA_ERROR, DWF_TIMEOUT, DWF_BAD_ARG = 4, 5, 6
 OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD = 0, 1, 2, 3
-SOLVER_CG64, SOLVER_MIXED = 0, 1
+SOLVER_CG64, SOLVER_MIXED, SOLVER_EO_MIXED = 0, 1, 2
 
 
 class DwfParams(C.Structure):
@@ -27,7 +27,7 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("status", C.c_int),
                 ("solver", C.c_int), ("relres", C.c_double), ("true_relres", C.c_double),
                 ("reliable_updates", C.c_int), ("fallback", C.c_int),
-                ("dirac_relres", C.c_double)]
+                ("dirac_relres", C.c_double), ("schur_iterations", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -105,7 +105,7 @@ SIGNATURES = {
     "wil_solve_cgnr": (_I, [_P, _P, _P, _D, _I, _I, _P, _P]),
     "wil_solve_dddag": (_I, [_P, _P, _P, _D, _I, _I, _P, _P]),
     "wil_hmc_step": (_I, [_P, C.POINTER(HmcParams), _P, _P, _P, _D, _P, C.POINTER(TrajInfo)]),
-    "dwf_solver_kernel_ms": (C.c_double, [_P, C.POINTER(C.c_uint64)]),
+    "dwf_solver_kernel_ms": (C.c_double, [_P, _I, C.POINTER(C.c_uint64)]),
 }
 
 _lib = None

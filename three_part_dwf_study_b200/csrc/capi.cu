@@ -282,8 +282,8 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     CK(cudaStreamSynchronize(c->stream));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    c->solver_ms += ms;
-    c->solver_launches += 1;
+    c->solver_ms[0] += ms;
+    c->solver_launches[0] += 1;
     if (hb.err != 0)
         return ctx_fail(c, hb.err, hb.err == DWF_TIMEOUT ? "persistent solver: a grid barrier wait ran out"
                                                           : "persistent solver: device error");
@@ -298,8 +298,11 @@ int solve_batch(dwf_ctx* c, int op, int nrhs, const int* conf_h, const double2* 
 {
     if (op != DWF_OP_DDDAG && op != DWF_OP_DDAGD)
         return ctx_fail(c, DWF_BAD_ARG, "cg: op must be DWF_OP_DDDAG or DWF_OP_DDAGD");
-    if (nrhs < 1 || maxiter < 0 || !(rtol >= 0.0) || (solver != DWF_SOLVER_CG64 && solver != DWF_SOLVER_MIXED))
+    if (nrhs < 1 || maxiter < 0 || !(rtol >= 0.0) ||
+        (solver != DWF_SOLVER_CG64 && solver != DWF_SOLVER_MIXED && solver != DWF_SOLVER_EO_MIXED))
         return ctx_fail(c, DWF_BAD_ARG, "cg: bad nrhs, maxiter, rtol or solver");
+    if (solver == DWF_SOLVER_EO_MIXED)
+        solver = DWF_SOLVER_MIXED;  // a general right-hand side has no source to precondition
     if (c->nconf < 1)
         return ctx_fail(c, DWF_BAD_ARG, "cg: no gauge configuration (set_gauge first)");
     for (int k = 0; conf_h && k < nrhs; ++k)
@@ -372,6 +375,7 @@ int solve_batch(dwf_ctx* c, int op, int nrhs, const int* conf_h, const double2* 
             I.reliable_updates = ru[k];
             I.fallback = fallback[k];
             I.dirac_relres = 0.0;
+            I.schur_iterations = 0;
             if (!std::isfinite(tr[k]) && I.status == DWF_OK)
                 I.status = DWF_NONFINITE;
         }
@@ -424,10 +428,35 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
         if (st)
             return st;
     }
-    st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 0, rtol, maxiter, solver,
-                     c->kind == 1 ? 1 : 0, info);
-    if (st)
-        return st;
+    if (solver == DWF_SOLVER_EO_MIXED && eo_eligible(c))
+    {
+        // Even-odd Schur solve of D x = src as the starting point, then the
+        // full-lattice mixed solve on D^dag D from it: the reference's
+        // stopping rule |D^dag D x - D^dag src| <= rtol |D^dag src| decides.
+        std::vector<int> eo_it, eo_ru;
+        st = propagators_eo(c, nrhs, conf_h, src, x, 0.3 * rtol, maxiter, eo_it, eo_ru);
+        if (st)
+            return st;
+        st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 1, rtol, maxiter,
+                         DWF_SOLVER_MIXED, 0, info);
+        if (st)
+            return st;
+        for (int k = 0; info && k < nrhs; ++k)
+        {
+            info[k].iterations += eo_it[k];
+            info[k].schur_iterations = eo_it[k];
+            info[k].reliable_updates += eo_ru[k];
+            info[k].solver = DWF_SOLVER_EO_MIXED;
+        }
+    }
+    else
+    {
+        st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 0, rtol, maxiter,
+                         solver == DWF_SOLVER_EO_MIXED ? DWF_SOLVER_MIXED : solver,
+                         c->kind == 1 ? 1 : 0, info);
+        if (st)
+            return st;
+    }
     for (int k0 = 0; k0 < nrhs; k0 += 65535)
     {
         const int n = std::min(65535, nrhs - k0);
@@ -736,13 +765,13 @@ int dwf_barrier_selftest(dwf_ctx* c, int missing_blocks, uint64_t limit_ns)
     return DWF_OK;
 }
 
-double dwf_solver_kernel_ms(const dwf_ctx* c, uint64_t* nlaunch)
+double dwf_solver_kernel_ms(const dwf_ctx* c, int kind, uint64_t* nlaunch)
 {
-    if (!c)
+    if (!c || kind < 0 || kind > 1)
         return 0.0;
     if (nlaunch)
-        *nlaunch = c->solver_launches;
-    return c->solver_ms;
+        *nlaunch = c->solver_launches[kind];
+    return c->solver_ms[kind];
 }
 
 }  // extern "C"

@@ -21,8 +21,8 @@ struct dwf_ctx
     uint64_t launches = 0;  // kernels launched by this context
     // CUDA events bracketing each persistent solver launch on `stream`
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    double solver_ms = 0.0;  // accumulated device time of solver launches
-    uint64_t solver_launches = 0;
+    double solver_ms[2] = {0.0, 0.0};  // device time of solver launches: full lattice, even-odd
+    uint64_t solver_launches[2] = {0, 0};
 
     // gauge configurations
     int nconf = 0;
@@ -55,6 +55,23 @@ struct dwf_ctx
     int* w_ru = nullptr;
     double* w_true = nullptr;
     dwfb::GridBar* bar = nullptr;
+
+    // even-odd workspace (parity fields, allocated on first use)
+    int eo_rhs = 0;
+    double2* eo_se = nullptr;   // source, even sites
+    double2* eo_so = nullptr;   // source, odd sites
+    double2* eo_bh = nullptr;   // b_o - H_oe M5^-1 b_e
+    double2* eo_rhs_o = nullptr;  // Dhat^dag bhat
+    double2* eo_x = nullptr;    // odd solution
+    double2* eo_r = nullptr;
+    double2* eo_t = nullptr;
+    double2* eo_y = nullptr;    // even temporary
+    double2* eo_xn = nullptr;
+    float2* eo_r32 = nullptr;
+    float2* eo_p32 = nullptr;
+    float2* eo_t32 = nullptr;
+    float2* eo_y32 = nullptr;
+    float2* eo_e32 = nullptr;
 
     // HMC workspace (allocated on first use)
     double* h_mom = nullptr;    // [2V]
@@ -93,6 +110,11 @@ int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const 
               void* out, int precision);
 // Upload nconf configurations (host or device pointer) and recompute links.
 int set_gauge(dwf_ctx* c, int nconf, const double* theta, cudaMemcpyKind kind);
+// Even-odd preconditioned solve of D x = src for nrhs sources (device, full
+// lattice); returns DWF_BAD_ARG when the lattice does not allow it.
+int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
+                   double tol, int maxiter, std::vector<int>& iters, std::vector<int>& ru);
+bool eo_eligible(const dwf_ctx* c);
 // Propagator batch: x = (D^dag D)^-1 D^dag src on device fields.
 int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
                 double rtol, int maxiter, int solver, dwf_solve_info* info);

@@ -1,0 +1,202 @@
+// Host side of the even-odd preconditioned propagator solve.
+#include <algorithm>
+#include <vector>
+
+#include "context.cuh"
+#include "eo.cuh"
+
+using namespace dwfb;
+
+#define CK(call)                                                                        \
+    do                                                                                  \
+    {                                                                                   \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return ctx_fail(c, DWF_CUDA_ERROR, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace dwfb {
+
+struct EoDesc
+{
+    SolveDesc d;
+    EoGeo g;
+    int nch4, ch4;
+    double2* y64;
+    float2* y32;
+    double2* xn64;
+};
+__global__ void eo_pack_kernel(Lat L, EoGeo g, const double2* full, double2* ev, double2* od,
+                               long nrhs);
+__global__ void eo_unpack_kernel(Lat L, EoGeo g, const double2* ev, const double2* od,
+                                 double2* full, long nrhs);
+template <bool DAG>
+__global__ void eo_hopinv_kernel(Lat L, EoGeo g, const double2* in, const double2* src,
+                                 double sgn, double2* out, const double2* U, long usz,
+                                 const int* conf, long nrhs);
+template <bool DAG>
+__global__ void eo_combine_kernel(Lat L, EoGeo g, const double2* a, const double2* m,
+                                  const double2* y, double2* out, const double2* U, long usz,
+                                  const int* conf, long nrhs);
+__global__ void cg_eo_mixed_kernel(EoDesc e);
+
+bool eo_eligible(const dwf_ctx* c)
+{
+    return c->kind == 0 && c->L.Nt % 2 == 0 && c->L.Nx % 2 == 0 && c->L.diag >= 1.0;
+}
+
+namespace {
+
+int ensure_eo(dwf_ctx* c, int nrhs)
+{
+    if (nrhs <= c->eo_rhs)
+        return DWF_OK;
+    CK(cudaStreamSynchronize(c->stream));
+    void** bufs64[] = {reinterpret_cast<void**>(&c->eo_se), reinterpret_cast<void**>(&c->eo_so),
+                       reinterpret_cast<void**>(&c->eo_bh), reinterpret_cast<void**>(&c->eo_rhs_o),
+                       reinterpret_cast<void**>(&c->eo_x), reinterpret_cast<void**>(&c->eo_r),
+                       reinterpret_cast<void**>(&c->eo_t), reinterpret_cast<void**>(&c->eo_y),
+                       reinterpret_cast<void**>(&c->eo_xn)};
+    void** bufs32[] = {reinterpret_cast<void**>(&c->eo_r32), reinterpret_cast<void**>(&c->eo_p32),
+                       reinterpret_cast<void**>(&c->eo_t32), reinterpret_cast<void**>(&c->eo_y32),
+                       reinterpret_cast<void**>(&c->eo_e32)};
+    const size_t fh = size_t(nrhs) * c->L.nsite;  // complex entries of one parity field (2 * nsite / 2)
+    c->eo_rhs = 0;
+    for (void** b : bufs64)
+    {
+        if (*b)
+            cudaFree(*b);
+        *b = nullptr;
+        CK(cudaMalloc(b, fh * sizeof(double2)));
+    }
+    for (void** b : bufs32)
+    {
+        if (*b)
+            cudaFree(*b);
+        *b = nullptr;
+        CK(cudaMalloc(b, fh * sizeof(float2)));
+    }
+    c->eo_rhs = nrhs;
+    return DWF_OK;
+}
+
+}  // namespace
+
+int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
+                   double tol, int maxiter, std::vector<int>& iters, std::vector<int>& ru)
+{
+    if (!eo_eligible(c))
+        return ctx_fail(c, DWF_BAD_ARG, "even-odd solve needs even Nt, Nx and 3 - M5 >= 1");
+    constexpr int kMaxRhs = 2048;
+    iters.assign(nrhs, 0);
+    ru.assign(nrhs, 0);
+    EoGeo g{c->L.Nx / 2, c->L.V / 2};
+    const long fh = long(g.Vh) * c->L.Ls * 2;  // complex entries per parity field
+    const long fs = c->fsz();
+    for (int k0 = 0; k0 < nrhs; k0 += kMaxRhs)
+    {
+        const int n = std::min(kMaxRhs, nrhs - k0);
+        int st = ensure_workspace(c, n);
+        if (st || (st = ensure_eo(c, n)))
+            return st;
+        std::vector<int> conf(n, 0);
+        if (conf_h)
+            std::copy(conf_h + k0, conf_h + k0 + n, conf.begin());
+        CK(cudaMemcpyAsync(c->w_conf, conf.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        const int nb = std::max(1, 8 * c->nsm);
+        const long usz = c->usz();
+        // b_e, b_o; bhat = b_o - H_oe M5^-1 b_e; rhs = Dhat^dag bhat
+        eo_pack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, src + k0 * fs, c->eo_se, c->eo_so, n);
+        eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, nullptr, c->eo_se, 1.0, c->eo_y, c->U64, usz, c->w_conf, n);
+        eo_combine_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_so, nullptr, c->eo_y, c->eo_bh, c->U64, usz, c->w_conf, n);
+        eo_hopinv_kernel<true><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_bh, nullptr, 1.0, c->eo_y, c->U64, usz, c->w_conf, n);
+        eo_combine_kernel<true><<<nb, 256, 0, c->stream>>>(c->L, g, nullptr, c->eo_bh, c->eo_y, c->eo_rhs_o, c->U64, usz, c->w_conf, n);
+        CK(cudaGetLastError());
+        c->launches += 5;
+        CK(cudaMemsetAsync(c->eo_x, 0, size_t(n) * fh * sizeof(double2), c->stream));
+
+        EoDesc e{};
+        SolveDesc& d = e.d;
+        d.L = c->L;
+        d.L.nsite = g.Vh * c->L.Ls;  // persistent sweeps run over odd 5-D sites
+        d.nrhs = n;
+        d.fsz = fh;
+        d.rhs_conf = c->w_conf;
+        d.U64 = c->U64;
+        d.U32 = c->U32;
+        d.usz = usz;
+        d.b = c->eo_rhs_o;
+        d.x = c->eo_x;
+        d.r = c->eo_r;
+        d.t = c->eo_t;
+        d.r32 = c->eo_r32;
+        d.p32 = c->eo_p32;
+        d.t32 = c->eo_t32;
+        d.e32 = c->eo_e32;
+        d.rtol = tol;
+        d.maxiter = maxiter;
+        d.delta = 0.1;
+        d.stall_limit = 3;
+        d.out_iters = c->w_iters;
+        d.out_relres = c->w_relres;
+        d.out_status = c->w_status;
+        d.out_ru = c->w_ru;
+        d.bar = c->bar;
+        d.timeout_ns = c->timeout_ns;
+        e.g = g;
+        e.y64 = c->eo_y;
+        e.y32 = c->eo_y32;
+        e.xn64 = c->eo_xn;
+
+        const void* fn = reinterpret_cast<const void*>(&cg_eo_mixed_kernel);
+        const size_t smem = solver_smem_bytes(n);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int bps = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, 256, smem));
+        if (bps < 1)
+            return ctx_fail(c, DWF_CUDA_ERROR, "even-odd solver kernel cannot be resident");
+        const long cap = long(bps) * c->nsm;
+        int grid = 0;
+        choose_units(d.L.nsite, n, cap, &d.nch, &d.ch, &grid);
+        // 4-D even sites: enough units for every block, at least 32 sites each
+        e.nch4 = int(std::max<long>(1, std::min<long>(g.Vh / 32, (grid + n - 1) / n)));
+        e.ch4 = (g.Vh + e.nch4 - 1) / e.nch4;
+        e.nch4 = (g.Vh + e.ch4 - 1) / e.ch4;
+        st = ensure_part(c, size_t(n) * d.nch * 2);
+        if (st)
+            return st;
+        d.part = c->w_part;
+        d.expected_blocks = unsigned(grid);
+        CK(cudaMemsetAsync(c->bar, 0, sizeof(GridBar), c->stream));
+        void* args[] = {&e};
+        CK(cudaEventRecord(c->ev0, c->stream));
+        CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, smem, c->stream));
+        CK(cudaEventRecord(c->ev1, c->stream));
+        c->launches += 1;
+        std::vector<int> it(n), r(n);
+        GridBar hb{};
+        CK(cudaMemcpyAsync(it.data(), c->w_iters, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(r.data(), c->w_ru, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&hb, c->bar, sizeof(GridBar), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->solver_ms[1] += ms;
+        c->solver_launches[1] += 1;
+        if (hb.err != 0)
+            return ctx_fail(c, hb.err, "even-odd solver: grid barrier wait ran out");
+        for (int k = 0; k < n; ++k)
+        {
+            iters[k0 + k] = it[k];
+            ru[k0 + k] = r[k];
+        }
+        // x_e = M5^-1 (b_e - H_eo x_o); x = (x_e, x_o)
+        eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_x, c->eo_se, -1.0, c->eo_y, c->U64, usz, c->w_conf, n);
+        eo_unpack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_y, c->eo_x, x + k0 * fs, n);
+        CK(cudaGetLastError());
+        c->launches += 2;
+    }
+    return DWF_OK;
+}
+
+}  // namespace dwfb

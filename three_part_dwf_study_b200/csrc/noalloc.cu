@@ -212,6 +212,7 @@ extern "C" int dwf_cg_noalloc(const dwf_params* p, int op, const double* theta_d
         info->reliable_updates = 0;
         info->fallback = 0;
         info->dirac_relres = 0.0;
+        info->schur_iterations = 0;
     }
     return hi[1];
 }

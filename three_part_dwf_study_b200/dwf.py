@@ -311,9 +311,11 @@ class DomainWall:
     def launch_count(self):
         return int(A.lib().dwf_launch_count(self._h))
 
-    def solver_kernel_ms(self):
+    def solver_kernel_ms(self, kind=0):
+        """(ms, launches) of the persistent solver kernels of one kind:
+        0 full lattice, 1 even-odd."""
         n = C.c_uint64()
-        ms = A.lib().dwf_solver_kernel_ms(self._h, C.byref(n))
+        ms = A.lib().dwf_solver_kernel_ms(self._h, int(kind), C.byref(n))
         return ms, n.value
 
     def sync(self):

@@ -571,6 +571,27 @@ def profile_case():
     return 0
 
 
+def profile_dslash():
+    """Two applications of D at the Dslash bench lattice for each kernel
+    variant and precision (for ncu)."""
+    import torch
+    import three_part_dwf_study_b200 as T
+    from three_part_dwf_study_b200 import _capi as A
+    Dt, Dx, Dl = DSLASH_LATTICE
+    d = T.DomainWall(Dt, Dx, Dl, M5, MF, BETA)
+    d.set_gauge(np.random.default_rng(3).uniform(-np.pi, np.pi, 2 * Dt * Dx))
+    for dt in (torch.float64, torch.float32):
+        a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
+        b = torch.empty_like(a)
+        for v in (0, 1):
+            A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
+            for _ in range(2):
+                d.apply_dev(0, a, b)
+    d.sync()
+    d.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -580,9 +601,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
     ap.add_argument("--profile-case", action="store_true")
+    ap.add_argument("--profile-dslash", action="store_true")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
+    if args.profile_dslash:
+        return profile_dslash()
     if args.calibrate_reference:
         return calibrate_reference()
     if args.warmup < 3 and args.impl == "ours":

@@ -16,7 +16,9 @@
  *
  * Entry points whose name ends in _dev take device pointers (laid out the
  * same way, one right-hand side after another) and run on the context's
- * stream; the others take host pointers and copy.
+ * stream (dwf_stream); the caller orders that stream against the streams that
+ * produce the inputs and consume the outputs (e.g. cudaStreamWaitEvent both
+ * ways). The others take host pointers, copy, and return when done.
  *
  * Ownership: the caller owns every buffer it passes. A context owns its
  * device memory and stream. One context per host thread: a context is not
@@ -324,6 +326,15 @@ int dwf_cg_noalloc(const dwf_params* params, int op, const double* theta_dev, co
  * there are blocks. missing_blocks = 0 returns DWF_OK; > 0 makes every wait run
  * into limit_ns and returns DWF_TIMEOUT with the context still usable. */
 int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
+
+/* Dslash kernel variant for dwf_apply[_dev]: 0 = one thread per 5-D site,
+ * 1 = one thread per 4-D site sweeping the fifth dimension (links and fifth-
+ * dimension neighbours kept in registers), -1 = autotune (default): the first
+ * application per (precision, batch-size bucket) times both with CUDA events
+ * and keeps the faster. dwf_dslash_variant reports the choice in force for a
+ * precision and batch size (-1 if not tuned yet). */
+int dwf_set_dslash_variant(dwf_ctx* ctx, int variant);
+int dwf_dslash_variant(const dwf_ctx* ctx, int precision, int nrhs);
 
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);

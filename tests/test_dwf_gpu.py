@@ -197,3 +197,27 @@ def test_bounded_barrier_times_out_and_context_survives(tdwf):
     b = random_field(rng, d.Ndof)
     r = d.conjugate_gradient(3, th, b, rtol=1e-10, maxiter=2000)
     assert r.converged and r.info["true_relres"] < 1e-9
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("shape", [(8, 8, 4), (13, 37, 3), (64, 64, 16), (5, 3, 1), (16, 40, 24)])
+def test_dslash_variants_match_oracle(tdwf, variant, shape):
+    """Both Dslash kernels (one thread per 5-D site; one thread per 4-D site
+    sweeping the fifth dimension) in FP64 and FP32, ragged tile edges included."""
+    torch = pytest.importorskip("torch")
+    from three_part_dwf_study_b200 import _capi as A
+    Nt, Nx, Ls = shape
+    rng = np.random.default_rng(Nt * 7 + Nx * 3 + Ls)
+    d = tdwf.DomainWall(Nt, Nx, Ls, 1.2, 0.03)
+    o = O.Dwf(Nt, Nx, Ls, 1.2, 0.03)
+    assert A.lib().dwf_set_dslash_variant(d.handle, variant) == 0
+    th = random_theta(rng, Nt, Nx)
+    psi = random_field(rng, 2 * o.ndof)
+    for op, name in OPS:
+        ref = np.concatenate([o.apply(op, th, psi[:o.ndof]), o.apply(op, th, psi[o.ndof:])])
+        assert rel(d.apply(op, th, psi), ref) < 1e-13, name
+        x32 = torch.from_numpy(psi.astype(np.complex64)).cuda()
+        y32 = torch.empty_like(x32)
+        d.apply_dev(op, x32, y32)
+        assert rel(y32.cpu().numpy(), ref) < 2e-6, name
+    assert A.lib().dwf_dslash_variant(d.handle, 64, 2) == variant

@@ -84,6 +84,8 @@ SIGNATURES = {
     "dwf_propagators": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_propagators_dev": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_launch_count": (C.c_uint64, [_P]),
+    "dwf_set_dslash_variant": (_I, [_P, _I]),
+    "dwf_dslash_variant": (_I, [_P, _I, _I]),
     "dwf_barrier_selftest": (_I, [_P, _I, C.c_uint64]),
     "dwf_cg_noalloc": (_I, [C.POINTER(DwfParams), _I, _P, _P, _P, _I, _D, _I, _P,
                             C.POINTER(SolveInfo)]),

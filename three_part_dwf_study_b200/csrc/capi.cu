@@ -109,6 +109,80 @@ int ensure_part(dwf_ctx* c, size_t n)
     return st;
 }
 
+#ifndef DWFB_DIRAC_BLOCKS_PER_SM
+#define DWFB_DIRAC_BLOCKS_PER_SM 4  // grid cap of the site kernel (0: one site per thread)
+#endif
+
+namespace {
+
+// One application of D (dag = false) or D^dag with the chosen kernel variant.
+template <typename R>
+void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d, int conf0,
+                  const cplx<R>* in, cplx<R>* out, const cplx<R>* U)
+{
+    const long fs = c->fsz();
+    if (variant == 1)
+    {
+        const dim3 grid((c->L.Nx + 31) / 32, (c->L.Nt + 7) / 8, nrhs);
+        if (dag)
+            dirac_col_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        else
+            dirac_col_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+    }
+    else
+    {
+        const int nb = (c->L.nsite + 255) / 256;
+        const int bx = DWFB_DIRAC_BLOCKS_PER_SM > 0
+                           ? std::min(nb, std::max(1, DWFB_DIRAC_BLOCKS_PER_SM * c->nsm))
+                           : nb;
+        const dim3 grid(bx, nrhs);
+        if (dag)
+            dirac_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        else
+            dirac_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+    }
+    c->launches += 1;
+}
+
+// Autotuner: time both variants (two applications each, CUDA events on the
+// context stream) for this precision and batch-size bucket, keep the faster.
+template <typename R>
+int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<R>* in,
+                 cplx<R>* out, const cplx<R>* U)
+{
+    if (c->dslash_variant >= 0)
+        return c->dslash_variant;
+    int bucket = 0;
+    while ((1 << bucket) < nrhs && bucket < 20)
+        ++bucket;
+    const int key = (sizeof(R) == 8 ? 100 : 0) + bucket;
+    auto it = c->dslash_tuned.find(key);
+    if (it != c->dslash_tuned.end())
+        return it->second;
+    float best = 1e30f;
+    int choice = 0;
+    for (int v = 0; v < 2; ++v)
+    {
+        launch_dirac<R>(c, v, false, nrhs, conf_d, conf0, in, out, U);  // warm-up
+        cudaEventRecord(c->ev0, c->stream);
+        for (int k = 0; k < 2; ++k)
+            launch_dirac<R>(c, v, false, nrhs, conf_d, conf0, in, out, U);
+        cudaEventRecord(c->ev1, c->stream);
+        cudaEventSynchronize(c->ev1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        if (ms < best)
+        {
+            best = ms;
+            choice = v;
+        }
+    }
+    c->dslash_tuned[key] = choice;
+    return choice;
+}
+
+}  // namespace
+
 int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const void* in,
               void* out, int precision)
 {
@@ -116,10 +190,6 @@ int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const 
         return ctx_fail(c, DWF_BAD_ARG, "apply: bad op, nrhs or precision");
     if (conf0 < 0 || conf0 >= c->nconf)
         return ctx_fail(c, DWF_BAD_ARG, "apply: configuration index out of range (set_gauge first)");
-    const dim3 block(256);
-    const int bx = std::min((c->L.nsite + 255) / 256, std::max(1, 4 * c->nsm));
-    const dim3 grid(bx, nrhs);
-    const long fs = c->fsz();
     const bool two = (op == DWF_OP_DDDAG || op == DWF_OP_DDAGD);
     if (two)
     {
@@ -133,36 +203,21 @@ int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const 
     {
         const double2* src = static_cast<const double2*>(in);
         double2* mid = two ? c->w_t : static_cast<double2*>(out);
-        if (dag1)
-            dirac_kernel<true, double><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U64, c->usz(), conf_d, conf0);
-        else
-            dirac_kernel<false, double><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U64, c->usz(), conf_d, conf0);
+        const int v = pick_variant<double>(c, nrhs, conf_d, conf0, src, mid, c->U64);
+        launch_dirac<double>(c, v, dag1, nrhs, conf_d, conf0, src, mid, c->U64);
         if (two)
-        {
-            if (dag1)
-                dirac_kernel<false, double><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<double2*>(out), fs, c->U64, c->usz(), conf_d, conf0);
-            else
-                dirac_kernel<true, double><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<double2*>(out), fs, c->U64, c->usz(), conf_d, conf0);
-        }
+            launch_dirac<double>(c, v, !dag1, nrhs, conf_d, conf0, mid, static_cast<double2*>(out), c->U64);
     }
     else
     {
         const float2* src = static_cast<const float2*>(in);
         float2* mid = two ? c->w_t32 : static_cast<float2*>(out);
-        if (dag1)
-            dirac_kernel<true, float><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U32, c->usz(), conf_d, conf0);
-        else
-            dirac_kernel<false, float><<<grid, block, 0, c->stream>>>(c->L, src, mid, fs, c->U32, c->usz(), conf_d, conf0);
+        const int v = pick_variant<float>(c, nrhs, conf_d, conf0, src, mid, c->U32);
+        launch_dirac<float>(c, v, dag1, nrhs, conf_d, conf0, src, mid, c->U32);
         if (two)
-        {
-            if (dag1)
-                dirac_kernel<false, float><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<float2*>(out), fs, c->U32, c->usz(), conf_d, conf0);
-            else
-                dirac_kernel<true, float><<<grid, block, 0, c->stream>>>(c->L, mid, static_cast<float2*>(out), fs, c->U32, c->usz(), conf_d, conf0);
-        }
+            launch_dirac<float>(c, v, !dag1, nrhs, conf_d, conf0, mid, static_cast<float2*>(out), c->U32);
     }
     CK(cudaGetLastError());
-    c->launches += two ? 2 : 1;
     return DWF_OK;
 }
 
@@ -741,6 +796,29 @@ int dwf_propagators(dwf_ctx* c, int nrhs, const int* rhs_conf, const double* src
 }
 
 uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
+
+int dwf_set_dslash_variant(dwf_ctx* c, int variant)
+{
+    if (!c || variant < -1 || variant > 1)
+        return DWF_BAD_ARG;
+    c->dslash_variant = variant;
+    if (variant == -1)
+        c->dslash_tuned.clear();
+    return DWF_OK;
+}
+
+int dwf_dslash_variant(const dwf_ctx* c, int precision, int nrhs)
+{
+    if (!c || (precision != 64 && precision != 32) || nrhs < 1)
+        return -1;
+    if (c->dslash_variant >= 0)
+        return c->dslash_variant;
+    int bucket = 0;
+    while ((1 << bucket) < nrhs && bucket < 20)
+        ++bucket;
+    const auto it = c->dslash_tuned.find((precision == 64 ? 100 : 0) + bucket);
+    return it == c->dslash_tuned.end() ? -1 : it->second;
+}
 
 int dwf_barrier_selftest(dwf_ctx* c, int missing_blocks, uint64_t limit_ns)
 {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -19,6 +20,11 @@ struct dwf_ctx
     uint64_t timeout_ns = 5000000000ull;
     std::string err;
     uint64_t launches = 0;  // kernels launched by this context
+    // Dslash kernel variant: -1 autotune, 0 one thread per 5-D site, 1 one
+    // thread per 4-D site sweeping the fifth dimension; tuned choices cached
+    // per (precision, batch-size bucket).
+    int dslash_variant = -1;
+    std::map<int, int> dslash_tuned;
     // CUDA events bracketing each persistent solver launch on `stream`
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double solver_ms[2] = {0.0, 0.0};  // device time of solver launches: full lattice, even-odd

@@ -145,4 +145,80 @@ __device__ __forceinline__ void site_coords(const Lat& L, int i, int& s, int& t,
     x = r - t * L.Nx;
 }
 
+// The same operator computed by one thread for one 4-D site (t, x) and every
+// fifth-dimension slice: the four link phases are loaded once and reused for
+// all Ls slices, and the fifth-dimension hop takes psi(s-1), psi(s), psi(s+1)
+// from a rolling register window (each centre spinor is loaded once, as the
+// "next" of the previous slice). emit(s, out) receives each output spinor.
+template <bool DAG, typename R, typename Emit>
+__device__ __forceinline__ void dirac_column(const cplx<R>* __restrict__ in,
+                                             const cplx<R>* __restrict__ U, const Lat& L, int t,
+                                             int x, Emit emit)
+{
+    using T = cplx<R>;
+    const int Nt = L.Nt, Nx = L.Nx, V = L.V, Ls = L.Ls;
+    const int tp = (t + 1 == Nt) ? 0 : t + 1;
+    const int tm = (t == 0) ? Nt - 1 : t - 1;
+    const int xp = (x + 1 == Nx) ? 0 : x + 1;
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+    const int here = t * Nx + x;
+    const int itp = tp * Nx + x, itm = tm * Nx + x, ixp = t * Nx + xp, ixm = t * Nx + xm;
+    const T Ut = U[here];
+    const T Utm = U[itm];
+    const T Ux = U[V + here];
+    const T Uxm = U[V + t * Nx + xm];
+    const R stp = (t == Nt - 1) ? R(L.bct) : R(1);
+    const R stm = (t == 0) ? R(L.bct) : R(1);
+    const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
+    const R sxm = (x == 0) ? R(L.bcx) : R(1);
+    constexpr R kf = DAG ? R(1) : R(-1);
+    constexpr R kb = -kf;
+    const R dg = R(L.diag), mf = R(L.mf);
+    const Spinor<R> first = ld_spinor(in, here);
+    Spinor<R> prev = L.fifth ? ld_spinor(in, long(Ls - 1) * V + here) : first;
+    Spinor<R> cur = first;
+    for (int s = 0; s < Ls; ++s)
+    {
+        const long sb = long(s) * V;
+        const Spinor<R> next = (s + 1 < Ls) ? ld_spinor(in, sb + V + here) : first;
+        const Spinor<R> vtp = ld_spinor(in, sb + itp);
+        const Spinor<R> vtm = ld_spinor(in, sb + itm);
+        const Spinor<R> vxp = ld_spinor(in, sb + ixp);
+        const Spinor<R> vxm = ld_spinor(in, sb + ixm);
+        T w = cmul(Ut, stp * (vtp.s0 + kf * vtp.s1));
+        T up = w;
+        T lo = kf * w;
+        w = cmulc(Utm, stm * (vtm.s0 + kb * vtm.s1));
+        up += w;
+        lo += kb * w;
+        w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
+        up += w;
+        lo += kf * itimes(w);
+        w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
+        up += w;
+        lo += kb * itimes(w);
+        Spinor<R> o{dg * cur.s0 - R(0.5) * up, dg * cur.s1 - R(0.5) * lo};
+        if (L.fifth)
+        {
+            // D: spin 1 from s+1 (m_f psi(0) at the top), spin 0 from s-1 (m_f psi(Ls-1) at 0);
+            // D^dag: the directions swapped.
+            const R cup = (s + 1 == Ls) ? mf : R(-1);
+            const R cdn = (s == 0) ? mf : R(-1);
+            if (!DAG)
+            {
+                o.s1 += cup * next.s1;
+                o.s0 += cdn * prev.s0;
+            }
+            else
+            {
+                o.s1 += cdn * prev.s1;
+                o.s0 += cup * next.s0;
+            }
+        }
+        emit(s, o);
+        prev = cur;
+        cur = next;
+    }
+}
+
 }  // namespace dwfb

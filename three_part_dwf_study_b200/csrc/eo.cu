@@ -143,7 +143,11 @@ template __global__ void eo_combine_kernel<true>(Lat, EoGeo, const double2*, con
 
 // ---- persistent mixed-precision Schur CG ------------------------------------
 
-__global__ void __launch_bounds__(256, 3) cg_eo_mixed_kernel(EoDesc e)
+#ifndef DWFB_EO_MINB
+#define DWFB_EO_MINB 3  // resident 256-thread blocks per SM the register budget targets
+#endif
+
+__global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e)
 {
     const SolveDesc& d = e.d;
     const EoGeo g = e.g;

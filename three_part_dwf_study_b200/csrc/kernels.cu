@@ -36,6 +36,36 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// One thread per 4-D site, all Ls slices (links and the fifth-dimension
+// neighbours reused from registers); blocks are 32 x 8 tiles of (x, t) so the
+// t +- 1 neighbours of a warp are mostly loaded by the block's other warps.
+template <bool DAG, typename R>
+__global__ void __launch_bounds__(256)
+    dirac_col_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out, long fsz,
+                     const cplx<R>* __restrict__ U, long usz, const int* __restrict__ conf,
+                     int conf0)
+{
+    const int j = blockIdx.z;
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int t = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= L.Nx || t >= L.Nt)
+        return;
+    const int c = conf ? conf[j] : conf0;
+    cplx<R>* outj = out + j * fsz;
+    const int here = t * L.Nx + x;
+    dirac_column<DAG, R>(in + j * fsz, U + long(c) * usz, L, t, x,
+                         [&](int s, const Spinor<R>& o) { st_spinor(outj, long(s) * L.V + here, o); });
+}
+
+template __global__ void dirac_col_kernel<false, double>(Lat, const double2*, double2*, long,
+                                                         const double2*, long, const int*, int);
+template __global__ void dirac_col_kernel<true, double>(Lat, const double2*, double2*, long,
+                                                        const double2*, long, const int*, int);
+template __global__ void dirac_col_kernel<false, float>(Lat, const float2*, float2*, long,
+                                                        const float2*, long, const int*, int);
+template __global__ void dirac_col_kernel<true, float>(Lat, const float2*, float2*, long,
+                                                       const float2*, long, const int*, int);
+
 template __global__ void dirac_kernel<false, double>(Lat, const double2*, double2*, long,
                                                      const double2*, long, const int*, int);
 template __global__ void dirac_kernel<true, double>(Lat, const double2*, double2*, long,

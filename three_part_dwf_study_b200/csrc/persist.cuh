@@ -6,8 +6,14 @@
 
 #include "solver.cuh"
 
+#ifndef DWFB_SWEEP_UNROLL
+#define DWFB_SWEEP_UNROLL 1  // sites per thread whose loads the sweep loop may overlap
+#endif
+
 namespace dwfb {
 namespace persist {
+
+constexpr int kSweepUnroll = DWFB_SWEEP_UNROLL;
 
 struct Smem
 {
@@ -109,6 +115,7 @@ __device__ void sweep_sites(const SolveDesc& d, const int* act, int nact, int ns
         const int end = min(beg + ch, nsite);
         const long uo = long(d.rhs_conf[j]) * d.usz;  // this unit's link offset
         double a0 = 0.0, a1 = 0.0;
+#pragma unroll kSweepUnroll
         for (int i = beg + threadIdx.x; i < end; i += blockDim.x)
         {
             const double2 v = f(j, i, uo);

@@ -129,6 +129,29 @@ class DomainWall:
         return CgResult(x, info.iterations, info.relres, bool(info.converged), info.as_dict())
 
     # ---- device entry points (torch tensors) -----------------------------------------
+    def _ordered(self):
+        """Context manager: the library's stream waits for the work already
+        queued on torch's current stream (the tensors' producers), and torch's
+        current stream waits for the library's work before anything reads the
+        results."""
+        import contextlib
+        import torch
+
+        @contextlib.contextmanager
+        def cm():
+            cur = torch.cuda.current_stream()
+            ext = torch.cuda.ExternalStream(self.stream_ptr())
+            e0 = torch.cuda.Event()
+            e0.record(cur)
+            ext.wait_event(e0)
+            try:
+                yield
+            finally:
+                e1 = torch.cuda.Event()
+                e1.record(ext)
+                cur.wait_event(e1)
+        return cm()
+
     def _dev_fields(self, t, what):
         """(precision, nrhs) of a contiguous CUDA tensor holding whole fields.
         float64/complex128 -> FP64, float32/complex64 -> FP32; the byte count
@@ -155,7 +178,8 @@ class DomainWall:
         n = thetas.numel() // self.Ngauge
         if n < 1 or n * self.Ngauge != thetas.numel():
             raise ValueError("thetas: size is not a multiple of 2*Nt*Nx")
-        self._check(A.lib().dwf_set_gauge_dev(self._h, n, C.c_void_p(thetas.data_ptr())))
+        with self._ordered():
+            self._check(A.lib().dwf_set_gauge_dev(self._h, n, C.c_void_p(thetas.data_ptr())))
         self._theta = None
 
     def apply_dev(self, op, inp, out, conf=0):
@@ -163,8 +187,9 @@ class DomainWall:
         prec2, nrhs2 = self._dev_fields(out, "out")
         if (prec, nrhs) != (prec2, nrhs2):
             raise ValueError("in/out: precision or field count differ")
-        self._check(A.lib().dwf_apply_dev(self._h, op, conf, C.c_void_p(inp.data_ptr()),
-                                          C.c_void_p(out.data_ptr()), nrhs, prec))
+        with self._ordered():
+            self._check(A.lib().dwf_apply_dev(self._h, op, conf, C.c_void_p(inp.data_ptr()),
+                                              C.c_void_p(out.data_ptr()), nrhs, prec))
 
     def cg_batch_dev(self, op, b, x, rhs_conf=None, has_guess=False, rtol=1e-10, maxiter=1000,
                      solver=A.SOLVER_CG64):
@@ -178,10 +203,11 @@ class DomainWall:
             conf = np.ascontiguousarray(rhs_conf, dtype=np.int32).reshape(-1)
             if conf.size != nrhs:
                 raise ValueError(f"rhs_conf: {conf.size} entries for {nrhs} right-hand sides")
-        self._check(A.lib().dwf_cg_batch_dev(
-            self._h, op, nrhs, _ptr(conf) if conf is not None else None,
-            C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), int(has_guess), float(rtol),
-            int(maxiter), int(solver), infos))
+        with self._ordered():
+            self._check(A.lib().dwf_cg_batch_dev(
+                self._h, op, nrhs, _ptr(conf) if conf is not None else None,
+                C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), int(has_guess),
+                float(rtol), int(maxiter), int(solver), infos))
         return [i.as_dict() for i in infos]
 
     def propagators(self, src, rhs_conf=None, rtol=1e-10, maxiter=10000, solver=A.SOLVER_MIXED):
@@ -215,9 +241,11 @@ class DomainWall:
             conf = np.ascontiguousarray(rhs_conf, dtype=np.int32).reshape(-1)
             if conf.size != nrhs:
                 raise ValueError("rhs_conf: wrong length")
-        self._check(A.lib().dwf_propagators_dev(
-            self._h, nrhs, _ptr(conf) if conf is not None else None, C.c_void_p(src.data_ptr()),
-            C.c_void_p(x.data_ptr()), float(rtol), int(maxiter), int(solver), infos))
+        with self._ordered():
+            self._check(A.lib().dwf_propagators_dev(
+                self._h, nrhs, _ptr(conf) if conf is not None else None,
+                C.c_void_p(src.data_ptr()), C.c_void_p(x.data_ptr()), float(rtol), int(maxiter),
+                int(solver), infos))
         return [i.as_dict() for i in infos]
 
     # ---- HMC pieces (reference names) -----------------------------------------------

@@ -75,7 +75,17 @@ typedef enum
      * reference's stopping rule on the full normal equation decides. Needs even
      * Nt, Nx and 3 - M5 >= 1 (else it runs DWF_SOLVER_MIXED); elsewhere it is
      * DWF_SOLVER_MIXED. */
-    DWF_SOLVER_EO_MIXED = 2
+    DWF_SOLVER_EO_MIXED = 2,
+    /* Propagator solves with the learned preconditioner (no counterpart in the
+     * reference; needs dwf_lp_init, normally followed by dwf_lp_train): FP64
+     * defect correction around an FP32 BiCGStab on D x = src, right-
+     * preconditioned by the gauge-equivariant network N ~ D^-1 (BF16 channel
+     * mixing, FP32 accumulation); the reference's stopping rule
+     * |D^dag (D x - src)| <= rtol |D^dag src| is checked on the FP64 true
+     * residual after each inner solve. A right-hand side whose true residual
+     * falls by less than a factor 2 in a cycle continues with DWF_SOLVER_MIXED
+     * (CG on D^dag D) from its iterate (info.fallback = 1). */
+    DWF_SOLVER_LEARNED = 3
 } dwf_solver;
 
 /* Domain-wall context parameters: the parameters.txt keys dwf.Nt, dwf.Nx,
@@ -101,7 +111,8 @@ typedef struct
     int fallback;        /* 1 if the mixed path fell back to FP64 CG */
     double dirac_relres; /* propagator solves: |D x - src| / |src| (correlator.hpp:225-227); else 0 */
     int schur_iterations;/* DWF_SOLVER_EO_MIXED: iterations of the even-odd stage (included
-                            in `iterations`); else 0 */
+                            in `iterations`); DWF_SOLVER_LEARNED: preconditioned BiCGStab
+                            iterations (2 network and 2 D applications each); else 0 */
 } dwf_solve_info;
 
 typedef struct dwf_ctx dwf_ctx;
@@ -343,8 +354,69 @@ uint64_t dwf_launch_count(const dwf_ctx* ctx);
  * CUDA events on the context stream; *nlaunch (optional) = their count. */
 double dwf_solver_kernel_ms(const dwf_ctx* ctx, int kind, uint64_t* nlaunch);
 
+/* ---- learned preconditioner (no counterpart in the reference) ------------------ */
+/* A gauge-equivariant parallel-transport convolution network N ~ D^-1 of four
+ * layers, C0 -> hidden -> hidden -> hidden -> C0 complex channels per 4-D site
+ * (C0 = 2 Ls for domain wall, channel 2 s + spin; 2 for Wilson). Layer:
+ *   out(y)[o] = sum_{k<9} sum_i W_k[o][i] * T_k(y) in(y + d_k)[i]
+ * over the 3x3 stencil offsets d_k = (dt, dx) in the order (0,0) (1,0) (-1,0)
+ * (0,1) (0,-1) (1,1) (1,-1) (-1,1) (-1,-1), T_k the U(1) transporter from
+ * y + d_k to y with the fermion boundary signs (diagonals: mean of the two
+ * two-link paths). No bias or activation, so N is linear and gauge covariant;
+ * N^dag runs the layers backwards with W'_k = (W_rev(k))^H. The transported
+ * values and the weights are rounded to BF16, the products accumulated in FP32
+ * on the tensor cores. Weights: 2 * dwf_lp_weights_size floats (re, im), layer
+ * by layer, each [9][cout][cin]. */
+int dwf_lp_init(dwf_ctx* ctx, int hidden, uint64_t seed);   /* hidden: 8, 16 or 32 */
+int dwf_lp_weights_size(const dwf_ctx* ctx, long* n_complex);
+int dwf_lp_get_weights(dwf_ctx* ctx, float* w);
+int dwf_lp_set_weights(dwf_ctx* ctx, const float* w);
+/* Transporters of configuration conf as the kernels use them: [V][9] complex float. */
+int dwf_lp_transports(dwf_ctx* ctx, int conf, float* T);
+/* out = N in (adjoint != 0: N^dag in) for nrhs FP32 complex fields in the
+ * operator layout on the device; rhs_conf as for dwf_cg_batch_dev. */
+int dwf_lp_apply_dev(dwf_ctx* ctx, int adjoint, int nrhs, const int* rhs_conf, const void* in_dev,
+                     void* out_dev);
+/* One layer (adjoint: its adjoint) on FP32 fields in the network layout [V][C]. */
+int dwf_lp_layer_dev(dwf_ctx* ctx, int layer, int adjoint, int nrhs, const int* rhs_conf,
+                     const void* in_dev, void* out_dev);
+/* Training loss (1/B) sum_b |N rho_b - e_b|^2 / |e_b|^2 over npair FP32 pairs
+ * (device, operator layout) and its gradient dL/dRe W + i dL/dIm W (host, as
+ * the weights; may be NULL). */
+int dwf_lp_loss_grad_dev(dwf_ctx* ctx, int npair, const int* pair_conf, const void* rho_dev,
+                         const void* e_dev, double* loss, float* grad);
+typedef struct
+{
+    int steps;           /* Adam steps */
+    int batch;           /* pairs per step (<= 1024) */
+    double lr;           /* Adam learning rate */
+    int lr_decay_steps;  /* halve the rate every this many steps (0: constant) */
+    int pairs_per_conf;  /* pairs generated per gauge configuration of the context */
+    int solver_iters;    /* solver pairs: error of the CG iterate after this many iterations
+                            against the converged solution (0: Gaussian errors only) */
+    int solver_every;    /* groups of 16 pairs: every solver_every-th is a solver group */
+    int solver_maxiter;  /* iteration limit of the converged solve */
+    uint64_t seed;
+} dwf_lp_train_params;
+typedef struct
+{
+    double loss_first, loss_last;
+    int steps, npairs, solver_pairs;
+    double seconds_pairs, seconds_train;
+} dwf_lp_train_info;
+/* Generate pairs (rho = D e) on the context's configurations and train the
+ * network with Adam on the GPU; history (host, may be NULL) receives the loss
+ * of every step. */
+int dwf_lp_train(dwf_ctx* ctx, const dwf_lp_train_params* params, dwf_lp_train_info* info,
+                 double* history);
+/* Inner solve: stop at |r| <= inner_tol |r0| or inner_maxiter iterations;
+ * at most outer_max defect-correction cycles (defaults 1e-4, 400, 40). */
+int dwf_lp_set_solver(dwf_ctx* ctx, double inner_tol, int inner_maxiter, int outer_max);
+
+
 #ifdef __cplusplus
 }
 #endif
+
 
 #endif /* DWF_B200_H */

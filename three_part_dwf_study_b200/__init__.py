@@ -5,10 +5,11 @@ The CUDA library (_lib/libdwfb200.so) is built by ``build.py``; without it every
 compute entry point raises.
 """
 from . import _capi
-from ._capi import (OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD, SOLVER_CG64, SOLVER_MIXED, SOLVER_EO_MIXED, DwfError,
+from ._capi import (OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD, SOLVER_CG64, SOLVER_MIXED, SOLVER_EO_MIXED, SOLVER_LEARNED,
+                    DwfError,
                     LIB_PATH)
 from .dwf import DomainWall, CgResult
 from .wilson import Wilson
 
 __all__ = ["DomainWall", "Wilson", "CgResult", "DwfError", "OP_D", "OP_DDAG", "OP_DDDAG", "OP_DDAGD",
-           "SOLVER_CG64", "SOLVER_MIXED", "SOLVER_EO_MIXED", "LIB_PATH"]
+           "SOLVER_CG64", "SOLVER_MIXED", "SOLVER_EO_MIXED", "SOLVER_LEARNED", "LIB_PATH"]

@@ -14,7 +14,7 @@ LIB_PATH = Path(os.environ.get("DWF_B200_LIB", _PKG / "_lib" / "libdwfb200.so"))
 DWF_OK, DWF_NOT_CONVERGED, DWF_ZERO_DENOM, DWF_NONFINITE = 0, 1, 2, 3
 DWF_CUDA_ERROR, DWF_TIMEOUT, DWF_BAD_ARG = 4, 5, 6
 OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD = 0, 1, 2, 3
-SOLVER_CG64, SOLVER_MIXED, SOLVER_EO_MIXED = 0, 1, 2
+SOLVER_CG64, SOLVER_MIXED, SOLVER_EO_MIXED, SOLVER_LEARNED = 0, 1, 2, 3
 
 
 class DwfParams(C.Structure):
@@ -58,6 +58,22 @@ class MeasureParams(C.Structure):
     _fields_ = [("n_point_times", C.c_int), ("n_wall_times", C.c_int), ("n_noise", C.c_int),
                 ("max_momentum", C.c_int), ("rtol", C.c_double), ("maxiter", C.c_int),
                 ("solver", C.c_int)]
+
+
+class LpTrainParams(C.Structure):
+    _fields_ = [("steps", C.c_int), ("batch", C.c_int), ("lr", C.c_double),
+                ("lr_decay_steps", C.c_int), ("pairs_per_conf", C.c_int),
+                ("solver_iters", C.c_int), ("solver_every", C.c_int),
+                ("solver_maxiter", C.c_int), ("seed", C.c_uint64)]
+
+
+class LpTrainInfo(C.Structure):
+    _fields_ = [("loss_first", C.c_double), ("loss_last", C.c_double), ("steps", C.c_int),
+                ("npairs", C.c_int), ("solver_pairs", C.c_int), ("seconds_pairs", C.c_double),
+                ("seconds_train", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _P = C.c_void_p
@@ -108,6 +124,16 @@ SIGNATURES = {
     "wil_solve_dddag": (_I, [_P, _P, _P, _D, _I, _I, _P, _P]),
     "wil_hmc_step": (_I, [_P, C.POINTER(HmcParams), _P, _P, _P, _D, _P, C.POINTER(TrajInfo)]),
     "dwf_solver_kernel_ms": (C.c_double, [_P, _I, C.POINTER(C.c_uint64)]),
+    "dwf_lp_init": (_I, [_P, _I, C.c_uint64]),
+    "dwf_lp_weights_size": (_I, [_P, C.POINTER(C.c_long)]),
+    "dwf_lp_get_weights": (_I, [_P, _P]),
+    "dwf_lp_set_weights": (_I, [_P, _P]),
+    "dwf_lp_transports": (_I, [_P, _I, _P]),
+    "dwf_lp_apply_dev": (_I, [_P, _I, _I, _P, _P, _P]),
+    "dwf_lp_layer_dev": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "dwf_lp_loss_grad_dev": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double), _P]),
+    "dwf_lp_train": (_I, [_P, C.POINTER(LpTrainParams), C.POINTER(LpTrainInfo), _P]),
+    "dwf_lp_set_solver": (_I, [_P, _D, _I, _I]),
 }
 
 _lib = None

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "context.cuh"
+#include "learned.cuh"
 #include "kernels.cuh"
 
 using namespace dwfb;
@@ -471,6 +472,19 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
     if (st)
         return st;
     const long fs = c->fsz();
+    if (solver == DWF_SOLVER_LEARNED)
+    {
+        for (int k0 = 0; k0 < nrhs; k0 += 65535)
+        {
+            const int n = std::min(65535, nrhs - k0);
+            st = lp_solve(c, n, conf_h ? conf_h + k0 : nullptr, src + k0 * fs, x + k0 * fs, rtol,
+                          maxiter, info ? info + k0 : nullptr);
+            if (st)
+                return st;
+        }
+    }
+    else
+    {
     // rhs = D^dag src, per configuration, into w_b (chunks of up to 65535 fields)
     std::vector<int> conf(nrhs, 0);
     if (conf_h)
@@ -512,6 +526,10 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
         if (st)
             return st;
     }
+    }
+    std::vector<int> conf(nrhs, 0);
+    if (conf_h)
+        std::copy(conf_h, conf_h + nrhs, conf.begin());
     for (int k0 = 0; k0 < nrhs; k0 += 65535)
     {
         const int n = std::min(65535, nrhs - k0);
@@ -598,10 +616,13 @@ int dwf_ctx_destroy(dwf_ctx* c)
     cudaSetDevice(c->device);
     if (c->stream)
         cudaStreamSynchronize(c->stream);
+    lp_destroy(c);
     void* bufs[] = {c->h_mom, c->h_force, c->h_part, c->h_scal, c->h_chi, c->h_phi, c->h_eta,
                     c->h_xi, c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_p2, c->w_p32b, c->w_t, c->w_b, c->w_x,
                     c->w_r32, c->w_p32, c->w_t32, c->w_e32, c->w_src, c->w_part, c->w_conf, c->w_active,
-                    c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar};
+                    c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar,
+                    c->eo_se, c->eo_so, c->eo_bh, c->eo_rhs_o, c->eo_x, c->eo_r, c->eo_t, c->eo_y,
+                    c->eo_xn, c->eo_r32, c->eo_p32, c->eo_t32, c->eo_y32, c->eo_e32};
     for (void* b : bufs)
         if (b)
             cudaFree(b);
@@ -667,6 +688,7 @@ int set_gauge(dwf_ctx* c, int nconf, const double* theta, cudaMemcpyKind kind)
     c->launches += 1;
     CK(cudaStreamSynchronize(c->stream));
     c->nconf = nconf;
+    c->gauge_version += 1;
     return DWF_OK;
 }
 }  // namespace dwfb

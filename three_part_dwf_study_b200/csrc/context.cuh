@@ -19,6 +19,8 @@ struct dwf_ctx
     cudaStream_t stream = nullptr;
     uint64_t timeout_ns = 5000000000ull;
     std::string err;
+    uint64_t gauge_version = 0;  // bumped whenever the links change
+    struct LpNet* lp = nullptr;  // learned preconditioner (dwf_lp_init)
     uint64_t launches = 0;  // kernels launched by this context
     // Dslash kernel variant: -1 autotune, 0 one thread per 5-D site, 1 one
     // thread per 4-D site sweeping the fifth dimension; tuned choices cached

@@ -1,0 +1,1725 @@
+// Learned preconditioner: PTC network kernels (forward / adjoint layers on
+// the tensor cores, weight gradients, loss, Adam), GPU training on pairs that
+// the plain solver generates, and the preconditioned solve.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "learned.cuh"
+
+using namespace dwfb;
+
+#define CK(call)                                                                        \
+    do                                                                                  \
+    {                                                                                   \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return ctx_fail(c, DWF_CUDA_ERROR, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define ST(call)                 \
+    do                           \
+    {                            \
+        const int s_ = (call);   \
+        if (s_ != DWF_OK)        \
+            return s_;           \
+    } while (0)
+
+namespace dwfb {
+
+// Offsets (dt, dx) of the 3x3 stencil.
+__constant__ int kOffT[9] = {0, 1, -1, 0, 0, 1, 1, -1, -1};
+__constant__ int kOffX[9] = {0, 0, 0, 1, -1, 1, -1, 1, -1};
+
+// Field layout seen by a layer: complex element (rhs, site h, channel c) at
+// rhs * rs + h * hs + (c / cg) * sg + (c % cg). Operator layout (domain wall
+// ((s*Nt+t)*Nx+x)*2+spin, c = 2 s + spin): hs = 2, cg = 2, sg = 2V.
+// Network layout [V][C]: hs = C, cg = C, sg = 0.
+struct FieldLayout
+{
+    long rs;
+    int hs, cg, sg;
+};
+
+__host__ __device__ __forceinline__ long chan_off(const FieldLayout& f, int c)
+{
+    return long(c / f.cg) * f.sg + (c % f.cg);
+}
+
+// ---------------------------------------------------------------------------
+// transports
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 hop_t(const double2* U, const Lat& L, int t, int x, int sg)
+{
+    const int Nt = L.Nt, Nx = L.Nx;
+    t = (t % Nt + Nt) % Nt;
+    x = (x % Nx + Nx) % Nx;
+    if (sg > 0)
+    {
+        const double2 u = U[t * Nx + x];
+        const double s = (t == Nt - 1) ? L.bct : 1.0;
+        return make_double2(s * u.x, s * u.y);
+    }
+    const int tm = (t == 0) ? Nt - 1 : t - 1;
+    const double2 u = U[tm * Nx + x];
+    const double s = (t == 0) ? L.bct : 1.0;
+    return make_double2(s * u.x, -s * u.y);
+}
+
+__device__ __forceinline__ double2 hop_x(const double2* U, const Lat& L, int t, int x, int sg)
+{
+    const int Nt = L.Nt, Nx = L.Nx;
+    t = (t % Nt + Nt) % Nt;
+    x = (x % Nx + Nx) % Nx;
+    const double2* Ux = U + L.V;
+    if (sg > 0)
+    {
+        const double2 u = Ux[t * Nx + x];
+        const double s = (x == Nx - 1) ? L.bcx : 1.0;
+        return make_double2(s * u.x, s * u.y);
+    }
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+    const double2 u = Ux[t * Nx + xm];
+    const double s = (x == 0) ? L.bcx : 1.0;
+    return make_double2(s * u.x, -s * u.y);
+}
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// T[conf][h][k] (FP32) from the FP64 links of each configuration.
+__global__ void lp_transport_kernel(Lat L, const double2* __restrict__ U64, long usz, int nconf,
+                                    float2* __restrict__ T)
+{
+    const long n = long(nconf) * L.V;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const int cf = int(i / L.V);
+        const int h = int(i - long(cf) * L.V);
+        const int t = h / L.Nx, x = h - t * L.Nx;
+        const double2* U = U64 + cf * usz;
+        float2* out = T + i * 9;
+        out[0] = make_float2(1.f, 0.f);
+        for (int k = 1; k < 9; ++k)
+        {
+            const int dt = kOffT[k], dx = kOffX[k];
+            double2 v;
+            if (dx == 0)
+                v = hop_t(U, L, t, x, dt);
+            else if (dt == 0)
+                v = hop_x(U, L, t, x, dx);
+            else
+            {
+                const double2 p1 = zmul(hop_t(U, L, t, x, dt), hop_x(U, L, t + dt, x, dx));
+                const double2 p2 = zmul(hop_x(U, L, t, x, dx), hop_t(U, L, t, x + dx, dt));
+                v = make_double2(0.5 * (p1.x + p2.x), 0.5 * (p1.y + p2.y));
+            }
+            out[k] = make_float2(float(v.x), float(v.y));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// weight packing into mma.m16n8k16 B fragments
+// ---------------------------------------------------------------------------
+// The complex contraction out[o] = sum_j W[o][j] a[j] is the real product of
+// A = [re a_j, im a_j]_j (interleaved) with B[2j][2o] = Re W, B[2j+1][2o] = -Im W,
+// B[2j][2o+1] = Im W, B[2j+1][2o+1] = Re W. Fragment of lane (g = lane/4,
+// q = lane%4) for k-step ks and n-tile nt: real column n = 8 nt + g (output
+// o = n/2, part n%2), rows of activations j = 8 ks + q (b0) and j + 4 (b1),
+// low half the row of Re a_j.
+__device__ __forceinline__ uint32_t pack_bf2(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__global__ void lp_pack_kernel(const float2* __restrict__ W, int cin, int cout, int adjoint,
+                               int ksteps, int nt, uint2* __restrict__ B)
+{
+    // layer dimensions as seen by the packed (possibly adjoint) layer
+    const int ci = adjoint ? cout : cin;
+    const int co = adjoint ? cin : cout;
+    const int total = ksteps * nt * 32;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x)
+    {
+        const int lane = idx & 31;
+        const int tile = idx >> 5;
+        const int ks = tile / nt, ntile = tile - ks * nt;
+        const int g = lane >> 2, q = lane & 3;
+        const int n = 8 * ntile + g;
+        const int o = n >> 1, part = n & 1;
+        uint32_t r[2];
+        for (int h = 0; h < 2; ++h)
+        {
+            const int j = 8 * ks + q + 4 * h;
+            float2 w = make_float2(0.f, 0.f);
+            if (o < co && j < 9 * ci)
+            {
+                const int k = j / ci, i = j - k * ci;
+                if (!adjoint)
+                    w = W[(long(k) * cout + o) * cin + i];
+                else
+                {
+                    // W'_k[o][i] = conj(W_rev(k)[i][o])
+                    const int kr = (k == 0) ? 0 : ((k <= 4) ? ((k & 1) ? k + 1 : k - 1) : 13 - k);
+                    const float2 u = W[(long(kr) * cout + i) * cin + o];
+                    w = make_float2(u.x, -u.y);
+                }
+            }
+            r[h] = part == 0 ? pack_bf2(w.x, -w.y) : pack_bf2(w.y, w.x);
+        }
+        B[idx] = make_uint2(r[0], r[1]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PTC layer on the tensor cores
+// ---------------------------------------------------------------------------
+struct PtcArgs
+{
+    const float2* in;
+    float2* out;
+    FieldLayout li, lo;
+    int cin, cout, ksteps;
+    const uint2* B;
+    const float2* T;
+    const int* conf;
+    int conf0;
+    int Nt, Nx, V, nrhs;
+};
+
+constexpr int kPtcWarps = 4;
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// bf16 pair of T * v, the complex product rounded per operation (no FMA), so
+// that the rounding to BF16 sees exactly the FP32 value the oracle computes.
+__device__ __forceinline__ uint32_t transported(float2 T, float2 v)
+{
+    const float re = __fsub_rn(__fmul_rn(T.x, v.x), __fmul_rn(T.y, v.y));
+    const float im = __fadd_rn(__fmul_rn(T.x, v.y), __fmul_rn(T.y, v.x));
+    return pack_bf2(re, im);
+}
+
+__host__ __device__ __forceinline__ size_t ptc_smem_bytes(int ksteps, int nt)
+{
+    return size_t(ksteps) * nt * 32 * sizeof(uint2) + size_t(16) * ksteps * sizeof(int) +
+           size_t(kPtcWarps) * 144 * (sizeof(int) + sizeof(float2));
+}
+
+// One warp computes 16 sites x all output channels of one right-hand side per
+// tile: A fragments are gathered straight from global memory (neighbour
+// value times transporter, rounded to BF16), B fragments come from shared memory.
+template <int NT>
+__global__ void __launch_bounds__(kPtcWarps * 32) lp_ptc_kernel(PtcArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2* Bs = reinterpret_cast<uint2*>(smem);
+    const int nb_frag = a.ksteps * NT * 32;
+    float2* Tsh = reinterpret_cast<float2*>(Bs + nb_frag);        // [warps][144]
+    int* kd = reinterpret_cast<int*>(Tsh + kPtcWarps * 144);     // [8 ksteps]
+    int* co = kd + 8 * a.ksteps;                                  // [8 ksteps]
+    int* nbs = co + 8 * a.ksteps;                                 // [warps][144]
+    for (int i = threadIdx.x; i < nb_frag; i += blockDim.x)
+        Bs[i] = a.B[i];
+    for (int j = threadIdx.x; j < 8 * a.ksteps; j += blockDim.x)
+    {
+        if (j < 9 * a.cin)
+        {
+            const int k = j / a.cin, c = j - k * a.cin;
+            kd[j] = k;
+            co[j] = int(chan_off(a.li, c));
+        }
+        else
+        {
+            kd[j] = 0;  // padding: any finite value, its weights are zero
+            co[j] = 0;
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    float2* wT = Tsh + warp * 144;
+    int* wnb = nbs + warp * 144;
+    const int tiles_per_rhs = (a.V + 15) / 16;
+    const long ntiles = long(tiles_per_rhs) * a.nrhs;
+    for (long tile = long(blockIdx.x) * kPtcWarps + warp; tile < ntiles;
+         tile += long(gridDim.x) * kPtcWarps)
+    {
+        const int rhs = int(tile / tiles_per_rhs);
+        const int h0 = int(tile - long(rhs) * tiles_per_rhs) * 16;
+        const int cf = a.conf ? a.conf[rhs] : a.conf0;
+        const float2* Tc = a.T + long(cf) * a.V * 9;
+        __syncwarp();
+        for (int e = lane; e < 144; e += 32)
+        {
+            const int r = e / 9, k = e - 9 * (e / 9);
+            const int h = h0 + r;
+            if (h < a.V)
+            {
+                const int t = h / a.Nx, x = h - t * a.Nx;
+                int tt = t + kOffT[k], xx = x + kOffX[k];
+                tt = tt < 0 ? tt + a.Nt : (tt >= a.Nt ? tt - a.Nt : tt);
+                xx = xx < 0 ? xx + a.Nx : (xx >= a.Nx ? xx - a.Nx : xx);
+                wnb[e] = (tt * a.Nx + xx) * a.li.hs;
+                wT[e] = Tc[long(h) * 9 + k];
+            }
+            else
+            {
+                wnb[e] = 0;
+                wT[e] = make_float2(0.f, 0.f);
+            }
+        }
+        __syncwarp();
+        const float2* inr = a.in + long(rhs) * a.li.rs;
+        float acc[NT][4];
+#pragma unroll
+        for (int n = 0; n < NT; ++n)
+            acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+        const int e0 = g * 9, e1 = (g + 8) * 9;
+        for (int ks = 0; ks < a.ksteps; ++ks)
+        {
+            const int j0 = 8 * ks + q, j1 = j0 + 4;
+            const int k0 = kd[j0], c0 = co[j0], k1 = kd[j1], c1 = co[j1];
+            const uint32_t A0 = transported(wT[e0 + k0], inr[wnb[e0 + k0] + c0]);
+            const uint32_t A1 = transported(wT[e1 + k0], inr[wnb[e1 + k0] + c0]);
+            const uint32_t A2 = transported(wT[e0 + k1], inr[wnb[e0 + k1] + c1]);
+            const uint32_t A3 = transported(wT[e1 + k1], inr[wnb[e1 + k1] + c1]);
+            const uint2* bp = Bs + ks * NT * 32 + lane;
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+            {
+                const uint2 b = bp[n * 32];
+                mma_bf16(acc[n], A0, A1, A2, A3, b.x, b.y);
+            }
+        }
+        float2* outr = a.out + long(rhs) * a.lo.rs;
+#pragma unroll
+        for (int n = 0; n < NT; ++n)
+        {
+            const int o = 4 * n + q;
+            if (o < a.cout)
+            {
+                const long off = chan_off(a.lo, o);
+                if (h0 + g < a.V)
+                    outr[long(h0 + g) * a.lo.hs + off] = make_float2(acc[n][0], acc[n][1]);
+                if (h0 + g + 8 < a.V)
+                    outr[long(h0 + g + 8) * a.lo.hs + off] = make_float2(acc[n][2], acc[n][3]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient: G_k[o][i] = sum_{rhs, y} g(y)[o] conj(a_k(y)[i])
+// ---------------------------------------------------------------------------
+struct GradArgs
+{
+    const float2* in;   // layer input
+    const float2* g;    // gradient at the layer output
+    FieldLayout li, lg;
+    int cin, cout;
+    const float2* T;
+    const int* conf;
+    int conf0;
+    int Nt, Nx, V, nrhs;
+    float2* part;  // [gridDim.x][9][cout][cin]
+};
+
+constexpr int kGradSites = 32;
+constexpr int kGradThreads = 256;
+constexpr int kGradMaxPer = 4;  // cout * cin <= kGradThreads * kGradMaxPer
+
+__global__ void __launch_bounds__(kGradThreads) lp_wgrad_kernel(GradArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2* gs = reinterpret_cast<float2*>(smem);      // [32][cout]
+    float2* as = gs + kGradSites * a.cout;             // [32][cin]
+    const int E = a.cout * a.cin;
+    float2 acc[9][kGradMaxPer];
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+#pragma unroll
+        for (int m = 0; m < kGradMaxPer; ++m)
+            acc[k][m] = make_float2(0.f, 0.f);
+    const int chunks_per_rhs = (a.V + kGradSites - 1) / kGradSites;
+    const long nchunks = long(chunks_per_rhs) * a.nrhs;
+    for (long chn = blockIdx.x; chn < nchunks; chn += gridDim.x)
+    {
+        const int rhs = int(chn / chunks_per_rhs);
+        const int h0 = int(chn - long(rhs) * chunks_per_rhs) * kGradSites;
+        const int cf = a.conf ? a.conf[rhs] : a.conf0;
+        const float2* Tc = a.T + long(cf) * a.V * 9;
+        const float2* inr = a.in + long(rhs) * a.li.rs;
+        const float2* gr = a.g + long(rhs) * a.lg.rs;
+        __syncthreads();
+        for (int e = threadIdx.x; e < kGradSites * a.cout; e += blockDim.x)
+        {
+            const int r = e / a.cout, o = e - r * a.cout;
+            const int h = h0 + r;
+            gs[e] = (h < a.V) ? gr[long(h) * a.lg.hs + chan_off(a.lg, o)] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+        {
+            __syncthreads();
+            for (int e = threadIdx.x; e < kGradSites * a.cin; e += blockDim.x)
+            {
+                const int r = e / a.cin, i = e - r * a.cin;
+                const int h = h0 + r;
+                float2 v = make_float2(0.f, 0.f);
+                if (h < a.V)
+                {
+                    const int t = h / a.Nx, x = h - t * a.Nx;
+                    int tt = t + kOffT[k], xx = x + kOffX[k];
+                    tt = tt < 0 ? tt + a.Nt : (tt >= a.Nt ? tt - a.Nt : tt);
+                    xx = xx < 0 ? xx + a.Nx : (xx >= a.Nx ? xx - a.Nx : xx);
+                    const float2 T = Tc[long(h) * 9 + k];
+                    const float2 u = inr[long(tt * a.Nx + xx) * a.li.hs + chan_off(a.li, i)];
+                    const uint32_t b = transported(T, u);
+                    const __nv_bfloat162 bb = *reinterpret_cast<const __nv_bfloat162*>(&b);
+                    v = __bfloat1622float2(bb);
+                }
+                as[e] = v;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < kGradMaxPer; ++m)
+            {
+                const int e = threadIdx.x + m * kGradThreads;
+                if (e < E)
+                {
+                    const int o = e / a.cin, i = e - o * a.cin;
+                    float2 s = acc[k][m];
+                    for (int r = 0; r < kGradSites; ++r)
+                    {
+                        const float2 gv = gs[r * a.cout + o];
+                        const float2 av = as[r * a.cin + i];
+                        // g * conj(a)
+                        s.x += gv.x * av.x + gv.y * av.y;
+                        s.y += gv.y * av.x - gv.x * av.y;
+                    }
+                    acc[k][m] = s;
+                }
+            }
+        }
+    }
+    float2* p = a.part + long(blockIdx.x) * 9 * E;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+#pragma unroll
+        for (int m = 0; m < kGradMaxPer; ++m)
+        {
+            const int e = threadIdx.x + m * kGradThreads;
+            if (e < E)
+                p[k * E + e] = acc[k][m];
+        }
+}
+
+// grad[e] = sum over blocks of part[b][e], in FP64 and block order.
+__global__ void lp_grad_reduce_kernel(const float2* __restrict__ part, int nblk, int n,
+                                      float2* __restrict__ grad)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    {
+        double sx = 0.0, sy = 0.0;
+        for (int b = 0; b < nblk; ++b)
+        {
+            const float2 v = part[long(b) * n + e];
+            sx += v.x;
+            sy += v.y;
+        }
+        grad[e] = make_float2(float(sx), float(sy));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// loss: (1/B) sum_b |out_b - e_b|^2 / |e_b|^2 and g = 2 (out - e) / (B |e_b|^2)
+// ---------------------------------------------------------------------------
+__global__ void lp_loss_partials_kernel(const float2* __restrict__ out, const float2* __restrict__ e,
+                                        long fsz, int nblk, double* __restrict__ part)
+{
+    __shared__ double red[32];
+    const int rhs = blockIdx.y;
+    const long ch = (fsz + nblk - 1) / nblk;
+    const long i0 = blockIdx.x * ch, i1 = (i0 + ch < fsz) ? i0 + ch : fsz;
+    double dd = 0.0, ee = 0.0;
+    for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+    {
+        const float2 o = out[rhs * fsz + i], t = e[rhs * fsz + i];
+        const double dx = double(o.x) - t.x, dy = double(o.y) - t.y;
+        dd += dx * dx + dy * dy;
+        ee += double(t.x) * t.x + double(t.y) * t.y;
+    }
+    dd = block_sum(dd, red);
+    ee = block_sum(ee, red);
+    if (threadIdx.x == 0)
+    {
+        part[(long(rhs) * nblk + blockIdx.x) * 2] = dd;
+        part[(long(rhs) * nblk + blockIdx.x) * 2 + 1] = ee;
+    }
+}
+
+// One thread per right-hand side: scale[b] = 2 / (B |e_b|^2), and (thread 0
+// after a block-wide pass) the loss.
+__global__ void lp_loss_finish_kernel(const double* __restrict__ part, int nrhs, int nblk,
+                                      double* __restrict__ scale, double* __restrict__ loss)
+{
+    __shared__ double terms[1024];
+    for (int b = threadIdx.x; b < nrhs; b += blockDim.x)
+    {
+        double dd = 0.0, ee = 0.0;
+        for (int j = 0; j < nblk; ++j)
+        {
+            dd += part[(long(b) * nblk + j) * 2];
+            ee += part[(long(b) * nblk + j) * 2 + 1];
+        }
+        scale[b] = 2.0 / (double(nrhs) * ee);
+        if (b < 1024)
+            terms[b] = dd / ee;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double s = 0.0;
+        for (int b = 0; b < nrhs && b < 1024; ++b)
+            s += terms[b];
+        *loss = s / nrhs;
+    }
+}
+
+__global__ void lp_loss_grad_kernel(const float2* __restrict__ out, const float2* __restrict__ e,
+                                    long fsz, int nrhs, const double* __restrict__ scale,
+                                    float2* __restrict__ g)
+{
+    const long n = fsz * nrhs;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const float s = float(scale[i / fsz]);
+        const float2 o = out[i], t = e[i];
+        g[i] = make_float2(s * (o.x - t.x), s * (o.y - t.y));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Adam on the FP32 master weights (real and imaginary parts separately)
+// ---------------------------------------------------------------------------
+__global__ void lp_adam_kernel(float* __restrict__ w, const float* __restrict__ g,
+                               float* __restrict__ m, float* __restrict__ v, long n, float lr,
+                               float b1, float b2, float c1, float c2, float eps)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gaussian fields from a counter-based generator (splitmix64 finaliser,
+// Box-Muller): each complex component N(0, 1/2), as the pseudofermion draws.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void lp_gauss_kernel(double2* __restrict__ out, long n, uint64_t seed)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const uint64_t r = mix64(seed ^ mix64(uint64_t(i)));
+        const double u1 = (double((r >> 11) & ((1ull << 26) - 1)) + 0.5) / double(1ull << 26);
+        const double u2 = double(r >> 37) / double(1ull << 27);
+        const double rad = sqrt(-log(u1));  // |z|^2 exponential with mean 1
+        double s, co;
+        sincospi(2.0 * u2, &s, &co);
+        out[i] = make_double2(rad * co, rad * s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// vector kernels of the solver (FP32 fields, FP64 dot products)
+// ---------------------------------------------------------------------------
+struct Dot
+{
+    const float2* a;
+    const float2* b;
+};
+
+// part[((slot * nrhs + rhs) * nblk + blk)] = <a, b> over this block's chunk,
+// for up to three pairs.
+__global__ void lp_dots_kernel(Dot d0, Dot d1, Dot d2, int ndot, long fsz, int nblk,
+                               double2* __restrict__ part)
+{
+    __shared__ double red[32];
+    const int rhs = blockIdx.y;
+    const int nrhs = gridDim.y;
+    const long ch = (fsz + nblk - 1) / nblk;
+    const long i0 = blockIdx.x * ch, i1 = (i0 + ch < fsz) ? i0 + ch : fsz;
+    const long base = long(rhs) * fsz;
+    for (int s = 0; s < ndot; ++s)
+    {
+        const Dot d = s == 0 ? d0 : (s == 1 ? d1 : d2);
+        double re = 0.0, im = 0.0;
+        for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+        {
+            const float2 x = d.a[base + i], y = d.b[base + i];
+            re += double(x.x) * y.x + double(x.y) * y.y;
+            im += double(x.x) * y.y - double(x.y) * y.x;
+        }
+        re = block_sum(re, red);
+        im = block_sum(im, red);
+        if (threadIdx.x == 0)
+            part[(long(s) * nrhs + rhs) * nblk + blockIdx.x] = make_double2(re, im);
+    }
+}
+
+__device__ __forceinline__ double2 sum_part(const double2* part, int slot, int nrhs, int rhs, int nblk)
+{
+    double re = 0.0, im = 0.0;
+    const double2* p = part + (long(slot) * nrhs + rhs) * nblk;
+    for (int b = 0; b < nblk; ++b)
+    {
+        re += p[b].x;
+        im += p[b].y;
+    }
+    return make_double2(re, im);
+}
+
+__device__ __forceinline__ double2 zdiv(double2 a, double2 b)
+{
+    const double d = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+
+__device__ __forceinline__ bool zfinite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+
+// Per-right-hand-side BiCGStab state.
+struct BsState
+{
+    double2 rho, alpha, omega, beta;
+    double rr;        // |r|^2 of the inner (normalised) system
+    int active;       // 1 while iterating
+    int breakdown;    // 1 once a denominator vanished
+    int iters;
+};
+
+// Coefficient steps: 0 start (rho = <rh, r> from slot 0, rr from slot 1),
+// 1 beta (rho1 = <rh, r>, rr = |r|^2 from slots 0, 1), 2 alpha (<rh, v> slot 0),
+// 3 omega (<t, s> slot 0, <t, t> slot 1). tgt2: |r|^2 at which a right-hand
+// side stops; maxit: inner iteration limit.
+__global__ void lp_bs_coef_kernel(int step, const double2* __restrict__ part, int nrhs, int nblk,
+                                  BsState* __restrict__ S, double tgt2, int maxit)
+{
+    const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rhs >= nrhs)
+        return;
+    BsState st = S[rhs];
+    if (step == 0)
+    {
+        st.rho = sum_part(part, 0, nrhs, rhs, nblk);
+        st.rr = sum_part(part, 1, nrhs, rhs, nblk).x;
+        st.alpha = make_double2(1.0, 0.0);
+        st.omega = make_double2(1.0, 0.0);
+        st.beta = make_double2(0.0, 0.0);
+        st.breakdown = 0;
+        st.iters = 0;
+        st.active = st.active && st.rr > tgt2;
+        S[rhs] = st;
+        return;
+    }
+    if (!st.active)
+    {
+        st.alpha = st.omega = st.beta = make_double2(0.0, 0.0);
+        S[rhs] = st;
+        return;
+    }
+    if (step == 1)
+    {
+        const double2 rho1 = sum_part(part, 0, nrhs, rhs, nblk);
+        st.rr = sum_part(part, 1, nrhs, rhs, nblk).x;
+        if (st.rr <= tgt2 || st.iters >= maxit)
+        {
+            st.active = 0;
+            st.alpha = st.omega = st.beta = make_double2(0.0, 0.0);
+            S[rhs] = st;
+            return;
+        }
+        // beta = (rho1 / rho) (alpha / omega)
+        const double2 b = zmul(zdiv(rho1, st.rho), zdiv(st.alpha, st.omega));
+        if (!zfinite(b) || (rho1.x == 0.0 && rho1.y == 0.0))
+        {
+            st.breakdown = 1;
+            st.active = 0;
+            st.alpha = st.omega = st.beta = make_double2(0.0, 0.0);
+        }
+        else
+        {
+            st.beta = b;
+            st.rho = rho1;
+        }
+        st.iters += 1;
+    }
+    else if (step == 2)
+    {
+        const double2 a = zdiv(st.rho, sum_part(part, 0, nrhs, rhs, nblk));
+        if (!zfinite(a))
+        {
+            st.breakdown = 1;
+            st.active = 0;
+            st.alpha = st.omega = st.beta = make_double2(0.0, 0.0);
+        }
+        else
+            st.alpha = a;
+    }
+    else
+    {
+        const double2 ts = sum_part(part, 0, nrhs, rhs, nblk);
+        const double tt = sum_part(part, 1, nrhs, rhs, nblk).x;
+        double2 w = make_double2(ts.x / tt, ts.y / tt);
+        if (!zfinite(w) || (w.x == 0.0 && w.y == 0.0))
+        {
+            // keep the alpha step (x += alpha ph, r = s), then stop
+            st.breakdown = 1;
+            w = make_double2(0.0, 0.0);
+        }
+        st.omega = w;
+    }
+    S[rhs] = st;
+}
+
+__device__ __forceinline__ float2 fz(double2 a) { return make_float2(float(a.x), float(a.y)); }
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// op 0: p = r + beta (p - omega v)
+// op 1: s = r - alpha v
+// op 2: x += alpha ph + omega sh ; r = s - omega t
+__global__ void lp_bs_vec_kernel(int op, long fsz, int nrhs, const BsState* __restrict__ S,
+                                 float2* __restrict__ p, const float2* __restrict__ r_in,
+                                 const float2* __restrict__ v, float2* __restrict__ s,
+                                 float2* __restrict__ x, const float2* __restrict__ ph,
+                                 const float2* __restrict__ sh, const float2* __restrict__ t,
+                                 float2* __restrict__ r_out)
+{
+    const long n = fsz * nrhs;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const BsState& st = S[i / fsz];
+        if (op == 0)
+        {
+            const float2 pv = p[i], vv = v[i], rv = r_in[i];
+            const float2 w = fz(st.omega), b = fz(st.beta);
+            const float2 d = make_float2(pv.x - (w.x * vv.x - w.y * vv.y), pv.y - (w.x * vv.y + w.y * vv.x));
+            const float2 bd = cmulf(b, d);
+            p[i] = make_float2(rv.x + bd.x, rv.y + bd.y);
+        }
+        else if (op == 1)
+        {
+            const float2 a = fz(st.alpha), vv = v[i], rv = r_in[i];
+            const float2 av = cmulf(a, vv);
+            s[i] = make_float2(rv.x - av.x, rv.y - av.y);
+        }
+        else
+        {
+            const float2 a = fz(st.alpha), w = fz(st.omega);
+            const float2 u1 = cmulf(a, ph[i]), u2 = cmulf(w, sh[i]);
+            const float2 xv = x[i];
+            x[i] = make_float2(xv.x + u1.x + u2.x, xv.y + u1.y + u2.y);
+            const float2 sv = s[i], wt = cmulf(w, t[i]);
+            r_out[i] = make_float2(sv.x - wt.x, sv.y - wt.y);
+        }
+    }
+}
+
+// Outer (FP64) steps.
+// r = b - Ax (tmp holds A x), partial |r|^2 into part (slot 0).
+__global__ void lp_resid_kernel(const double2* __restrict__ b, const double2* __restrict__ Ax,
+                                double2* __restrict__ r, long fsz, int nblk, double* __restrict__ part)
+{
+    __shared__ double red[32];
+    const int rhs = blockIdx.y;
+    const long ch = (fsz + nblk - 1) / nblk;
+    const long i0 = blockIdx.x * ch, i1 = (i0 + ch < fsz) ? i0 + ch : fsz;
+    double s = 0.0;
+    for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+    {
+        const long k = long(rhs) * fsz + i;
+        const double2 v = make_double2(b[k].x - Ax[k].x, b[k].y - Ax[k].y);
+        r[k] = v;
+        s += v.x * v.x + v.y * v.y;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0)
+        part[long(rhs) * nblk + blockIdx.x] = s;
+}
+
+__global__ void lp_norm_kernel(const double2* __restrict__ a, long fsz, int nblk, double* __restrict__ part)
+{
+    __shared__ double red[32];
+    const int rhs = blockIdx.y;
+    const long ch = (fsz + nblk - 1) / nblk;
+    const long i0 = blockIdx.x * ch, i1 = (i0 + ch < fsz) ? i0 + ch : fsz;
+    double s = 0.0;
+    for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+    {
+        const double2 v = a[long(rhs) * fsz + i];
+        s += v.x * v.x + v.y * v.y;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0)
+        part[long(rhs) * nblk + blockIdx.x] = s;
+}
+
+__global__ void lp_sum_kernel(const double* __restrict__ part, int nrhs, int nblk, double* __restrict__ out)
+{
+    const int rhs = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rhs >= nrhs)
+        return;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b)
+        s += part[long(rhs) * nblk + b];
+    out[rhs] = s;
+}
+
+// r32 = r64 * inv[rhs] (inv = 0 leaves a zero field)
+__global__ void lp_down_kernel(const double2* __restrict__ r, const double* __restrict__ inv, long fsz,
+                               int nrhs, float2* __restrict__ r32)
+{
+    const long n = fsz * nrhs;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const double s = inv[i / fsz];
+        r32[i] = make_float2(float(r[i].x * s), float(r[i].y * s));
+    }
+}
+
+// x += scale[rhs] * e32
+__global__ void lp_up_kernel(double2* __restrict__ x, const float2* __restrict__ e, const double* __restrict__ scale,
+                             long fsz, int nrhs)
+{
+    const long n = fsz * nrhs;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const double s = scale[i / fsz];
+        if (s != 0.0)
+            x[i] = make_double2(x[i].x + s * e[i].x, x[i].y + s * e[i].y);
+    }
+}
+
+__global__ void lp_f64_to_f32_kernel(const double2* __restrict__ a, float2* __restrict__ b, long n)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        b[i] = make_float2(float(a[i].x), float(a[i].y));
+}
+
+// e = x* - x_k (FP32)
+__global__ void lp_diff_kernel(const double2* __restrict__ a, const double2* __restrict__ b,
+                               float2* __restrict__ out, long n)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        out[i] = make_float2(float(a[i].x - b[i].x), float(a[i].y - b[i].y));
+}
+
+}  // namespace dwfb
+
+// ===========================================================================
+// host side
+// ===========================================================================
+struct LpNet
+{
+    int C0 = 0, H = 0;
+    int cin[kLpLayers], cout[kLpLayers], ksteps[kLpLayers], ntf[kLpLayers], nta[kLpLayers];
+    long woff[kLpLayers + 1];          // complex offsets of each layer's weights
+    long bf_off[kLpLayers + 1];        // uint2 offsets of forward fragments
+    long ba_off[kLpLayers + 1];        // and of adjoint fragments
+    float2* W = nullptr;               // FP32 master weights
+    float2* G = nullptr;               // gradient
+    float* m = nullptr;                // Adam moments (2 floats per complex weight)
+    float* v = nullptr;
+    long adam_t = 0;
+    uint2* Bf = nullptr;
+    uint2* Ba = nullptr;
+    float2* T = nullptr;               // transports [nconf][V][9]
+    int T_cap = 0;
+    uint64_t T_version = ~0ull;
+    // activations: layer inputs of the last forward pass (training)
+    int act_rhs = 0;
+    float2* act[kLpLayers] = {nullptr, nullptr, nullptr, nullptr};
+    float2* hid[2] = {nullptr, nullptr};
+    float2* gbuf[2] = {nullptr, nullptr};   // gradients flowing back (operator and hidden layout)
+    float2* gpart = nullptr;
+    size_t gpart_cap = 0;
+    int grad_blocks = 0;
+    double* lpart = nullptr;
+    double* lscale = nullptr;
+    double* dloss = nullptr;
+    size_t lpart_cap = 0;
+    int* dconf = nullptr;
+    int dconf_cap = 0;
+    // training pairs (FP32, operator layout)
+    int npairs = 0;
+    float2* pr_rho = nullptr;
+    float2* pr_e = nullptr;
+    std::vector<int> pr_conf;
+    // solver workspace
+    int s_rhs = 0;
+    float2* s_f32[9] = {};      // r, rh, p, v, s, t, ph, sh, x
+    double2* s_r64 = nullptr;
+    double2* s_t64 = nullptr;
+    double2* s_rhs64 = nullptr;
+    double2* s_part2 = nullptr;
+    double* s_part = nullptr;
+    double* s_val = nullptr;    // per-rhs scalars [4][nrhs]
+    BsState* s_state = nullptr;
+    // solver settings
+    double inner_tol = 1e-4;
+    int inner_max = 400;
+    int outer_max = 40;
+    long iters_total = 0;
+};
+
+namespace dwfb {
+namespace {
+
+template <typename T>
+int lp_grow(dwf_ctx* c, T*& p, size_t n)
+{
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    return DWF_OK;
+}
+
+int nt_of(int cout) { return (2 * cout + 7) / 8; }
+
+int grid_for(long n, int nsm) { return int(std::max<long>(1, std::min<long>((n + 255) / 256, 8L * nsm))); }
+
+int set_ptc_smem(dwf_ctx* c)
+{
+    static int done_dev = -1;
+    if (done_dev == c->device)
+        return DWF_OK;
+    const int mx = 200 * 1024;
+    CK(cudaFuncSetAttribute(lp_ptc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_ptc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_ptc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_ptc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_ptc_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    done_dev = c->device;
+    return DWF_OK;
+}
+
+// Pack the BF16 fragments of every layer (forward and adjoint) from W.
+int lp_pack(dwf_ctx* c)
+{
+    LpNet* n = c->lp;
+    for (int l = 0; l < kLpLayers; ++l)
+    {
+        const long nf = n->bf_off[l + 1] - n->bf_off[l];
+        const long na = n->ba_off[l + 1] - n->ba_off[l];
+        lp_pack_kernel<<<grid_for(nf, c->nsm), 256, 0, c->stream>>>(
+            n->W + n->woff[l], n->cin[l], n->cout[l], 0, n->ksteps[l], n->ntf[l], n->Bf + n->bf_off[l]);
+        // adjoint layer: cin' = cout, cout' = cin
+        lp_pack_kernel<<<grid_for(na, c->nsm), 256, 0, c->stream>>>(
+            n->W + n->woff[l], n->cin[l], n->cout[l], 1, (9 * n->cout[l] + 7) / 8, n->nta[l],
+            n->Ba + n->ba_off[l]);
+        c->launches += 2;
+    }
+    CK(cudaGetLastError());
+    return DWF_OK;
+}
+
+int lp_transports(dwf_ctx* c)
+{
+    LpNet* n = c->lp;
+    if (n->T_version == c->gauge_version && n->T_cap >= c->nconf)
+        return DWF_OK;
+    if (n->T_cap < c->nconf)
+    {
+        ST(lp_grow(c, n->T, size_t(c->nconf) * c->L.V * 9));
+        n->T_cap = c->nconf;
+    }
+    lp_transport_kernel<<<grid_for(long(c->nconf) * c->L.V, c->nsm), 256, 0, c->stream>>>(
+        c->L, c->U64, c->usz(), c->nconf, n->T);
+    c->launches += 1;
+    CK(cudaGetLastError());
+    n->T_version = c->gauge_version;
+    return DWF_OK;
+}
+
+int lp_conf(dwf_ctx* c, int nrhs, const int* conf_h, const int** conf_d)
+{
+    LpNet* n = c->lp;
+    if (nrhs > n->dconf_cap)
+    {
+        ST(lp_grow(c, n->dconf, nrhs));
+        n->dconf_cap = nrhs;
+    }
+    std::vector<int> cf(nrhs, 0);
+    if (conf_h)
+        std::copy(conf_h, conf_h + nrhs, cf.begin());
+    for (int k = 0; k < nrhs; ++k)
+        if (cf[k] < 0 || cf[k] >= c->nconf)
+            return ctx_fail(c, DWF_BAD_ARG, "learned: configuration index out of range");
+    CK(cudaMemcpyAsync(n->dconf, cf.data(), nrhs * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    *conf_d = n->dconf;
+    return DWF_OK;
+}
+
+FieldLayout op_layout(const dwf_ctx* c)
+{
+    // operator layout: channel c = 2 s + spin; a Wilson field is the Ls = 1 case
+    return FieldLayout{c->fsz(), 2, 2, 2 * c->L.V};
+}
+
+FieldLayout net_layout(const dwf_ctx* c, int C) { return FieldLayout{long(c->L.V) * C, C, C, 0}; }
+
+// One layer (forward or adjoint) on device fields.
+int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const float2* in,
+             FieldLayout li, float2* out, FieldLayout lo)
+{
+    LpNet* n = c->lp;
+    PtcArgs a;
+    a.in = in;
+    a.out = out;
+    a.li = li;
+    a.lo = lo;
+    a.cin = adjoint ? n->cout[l] : n->cin[l];
+    a.cout = adjoint ? n->cin[l] : n->cout[l];
+    a.ksteps = (9 * a.cin + 7) / 8;
+    a.B = adjoint ? n->Ba + n->ba_off[l] : n->Bf + n->bf_off[l];
+    a.T = n->T;
+    a.conf = conf_d;
+    a.conf0 = 0;
+    a.Nt = c->L.Nt;
+    a.Nx = c->L.Nx;
+    a.V = c->L.V;
+    a.nrhs = nrhs;
+    const int nt = nt_of(a.cout);
+    const size_t smem = ptc_smem_bytes(a.ksteps, nt);
+    const long ntiles = long((a.V + 15) / 16) * nrhs;
+    const int grid = int(std::max<long>(1, std::min<long>((ntiles + kPtcWarps - 1) / kPtcWarps, 3L * c->nsm)));
+    ST(set_ptc_smem(c));
+    switch (nt)
+    {
+    case 1: lp_ptc_kernel<1><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
+    case 2: lp_ptc_kernel<2><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
+    case 4: lp_ptc_kernel<4><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
+    case 8: lp_ptc_kernel<8><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
+    case 12: lp_ptc_kernel<12><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
+    default: return ctx_fail(c, DWF_BAD_ARG, "learned: unsupported channel count");
+    }
+    c->launches += 1;
+    CK(cudaGetLastError());
+    return DWF_OK;
+}
+
+int lp_ensure_act(dwf_ctx* c, int nrhs)
+{
+    LpNet* n = c->lp;
+    if (nrhs <= n->act_rhs)
+        return DWF_OK;
+    const size_t hid = size_t(nrhs) * c->L.V * n->H;
+    const size_t op = size_t(nrhs) * c->fsz();
+    for (int l = 1; l < kLpLayers; ++l)
+        ST(lp_grow(c, n->act[l], hid));
+    ST(lp_grow(c, n->hid[0], std::max(hid, op)));
+    ST(lp_grow(c, n->hid[1], std::max(hid, op)));
+    ST(lp_grow(c, n->gbuf[0], std::max(hid, op)));
+    ST(lp_grow(c, n->gbuf[1], std::max(hid, op)));
+    n->act_rhs = nrhs;
+    return DWF_OK;
+}
+
+// out = N in (adjoint: N^dag in), operator layout, FP32. Hidden fields in
+// hid[0], hid[1]; with `keep`, the layer inputs are also kept in act[] (act[0]
+// is `in` itself).
+int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* in, float2* out,
+           bool keep)
+{
+    LpNet* n = c->lp;
+    ST(lp_ensure_act(c, nrhs));
+    const FieldLayout lop = op_layout(c), lh = net_layout(c, n->H);
+    const float2* cur = in;
+    FieldLayout lcur = lop;
+    for (int s = 0; s < kLpLayers; ++s)
+    {
+        const int l = adjoint ? kLpLayers - 1 - s : s;
+        const bool last = (s == kLpLayers - 1);
+        float2* dst = last ? out : (keep ? n->act[s + 1] : n->hid[s & 1]);
+        if (keep)
+            n->act[0] = const_cast<float2*>(in);
+        ST(lp_layer(c, l, adjoint, nrhs, conf_d, cur, lcur, dst, last ? lop : lh));
+        cur = dst;
+        lcur = lh;
+    }
+    return DWF_OK;
+}
+
+int lp_ensure_lpart(dwf_ctx* c, size_t n)
+{
+    LpNet* L = c->lp;
+    if (n <= L->lpart_cap)
+        return DWF_OK;
+    ST(lp_grow(c, L->lpart, n));
+    L->lpart_cap = n;
+    return DWF_OK;
+}
+
+// Loss of the current network on pairs (rho, e) (device, operator layout),
+// the gradient into n->G. loss_out: host (may be null: stays on device).
+int lp_loss_grad(dwf_ctx* c, int nrhs, const int* conf_d, const float2* rho, const float2* e,
+                 double* loss_out)
+{
+    LpNet* n = c->lp;
+    ST(lp_ensure_act(c, nrhs));
+    const long fs = c->fsz();
+    // forward, keeping the layer inputs; output into gbuf[1]
+    float2* out = n->gbuf[1];
+    ST(lp_net(c, false, nrhs, conf_d, rho, out, true));
+    const int nblk = int(std::min<long>(64, (fs + 4095) / 4096));
+    ST(lp_ensure_lpart(c, size_t(nrhs) * nblk * 2));
+    if (!n->lscale)
+        ST(lp_grow(c, n->lscale, 65536));
+    if (!n->dloss)
+        ST(lp_grow(c, n->dloss, 1));
+    lp_loss_partials_kernel<<<dim3(nblk, nrhs), 256, 0, c->stream>>>(out, e, fs, nblk, n->lpart);
+    lp_loss_finish_kernel<<<1, 256, 0, c->stream>>>(n->lpart, nrhs, nblk, n->lscale, n->dloss);
+    float2* g = n->gbuf[0];
+    lp_loss_grad_kernel<<<grid_for(fs * nrhs, c->nsm), 256, 0, c->stream>>>(out, e, fs, nrhs, n->lscale, g);
+    c->launches += 3;
+    CK(cudaGetLastError());
+    // backward through the layers
+    const FieldLayout lop = op_layout(c), lh = net_layout(c, n->H);
+    const float2* gcur = g;
+    FieldLayout lg = lop;
+    const int nblk_g = std::max(1, std::min(2 * c->nsm, (c->L.V * nrhs + kGradSites - 1) / kGradSites));
+    long gmax = 0;
+    for (int l = 0; l < kLpLayers; ++l)
+        gmax = std::max<long>(gmax, 9L * n->cin[l] * n->cout[l]);
+    if (size_t(nblk_g) * gmax > n->gpart_cap)
+    {
+        ST(lp_grow(c, n->gpart, size_t(nblk_g) * gmax));
+        n->gpart_cap = size_t(nblk_g) * gmax;
+    }
+    for (int l = kLpLayers - 1; l >= 0; --l)
+    {
+        GradArgs a;
+        a.in = n->act[l];
+        a.g = gcur;
+        a.li = (l == 0) ? lop : lh;
+        a.lg = lg;
+        a.cin = n->cin[l];
+        a.cout = n->cout[l];
+        a.T = n->T;
+        a.conf = conf_d;
+        a.conf0 = 0;
+        a.Nt = c->L.Nt;
+        a.Nx = c->L.Nx;
+        a.V = c->L.V;
+        a.nrhs = nrhs;
+        a.part = n->gpart;
+        const size_t smem = size_t(kGradSites) * (a.cin + a.cout) * sizeof(float2);
+        lp_wgrad_kernel<<<nblk_g, kGradThreads, smem, c->stream>>>(a);
+        const int E = 9 * a.cin * a.cout;
+        lp_grad_reduce_kernel<<<(E + 255) / 256, 256, 0, c->stream>>>(n->gpart, nblk_g, E, n->G + n->woff[l]);
+        c->launches += 2;
+        CK(cudaGetLastError());
+        if (l > 0)
+        {
+            // gradient at this layer's input: the adjoint layer applied to g
+            float2* dst = (gcur == n->gbuf[0]) ? n->gbuf[1] : n->gbuf[0];
+            ST(lp_layer(c, l, true, nrhs, conf_d, gcur, lg, dst, lh));
+            gcur = dst;
+            lg = lh;
+        }
+    }
+    if (loss_out)
+    {
+        CK(cudaMemcpyAsync(loss_out, n->dloss, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return DWF_OK;
+}
+
+int lp_adam(dwf_ctx* c, double lr)
+{
+    LpNet* n = c->lp;
+    n->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const double c1 = 1.0 / (1.0 - std::pow(double(b1), double(n->adam_t)));
+    const double c2 = 1.0 / (1.0 - std::pow(double(b2), double(n->adam_t)));
+    const long nr = 2 * n->woff[kLpLayers];
+    lp_adam_kernel<<<grid_for(nr, c->nsm), 256, 0, c->stream>>>(
+        reinterpret_cast<float*>(n->W), reinterpret_cast<const float*>(n->G), n->m, n->v, nr,
+        float(lr), b1, b2, float(c1), float(c2), 1e-8f);
+    c->launches += 1;
+    CK(cudaGetLastError());
+    return lp_pack(c);
+}
+
+int lp_ensure_solver(dwf_ctx* c, int nrhs)
+{
+    LpNet* n = c->lp;
+    if (nrhs <= n->s_rhs)
+        return DWF_OK;
+    const size_t fs = size_t(nrhs) * c->fsz();
+    for (int k = 0; k < 9; ++k)
+        ST(lp_grow(c, n->s_f32[k], fs));
+    ST(lp_grow(c, n->s_r64, fs));
+    ST(lp_grow(c, n->s_t64, fs));
+    ST(lp_grow(c, n->s_rhs64, fs));
+    ST(lp_grow(c, n->s_part2, size_t(3) * nrhs * 64));
+    ST(lp_grow(c, n->s_part, size_t(nrhs) * 64));
+    ST(lp_grow(c, n->s_val, size_t(4) * nrhs));
+    ST(lp_grow(c, n->s_state, size_t(nrhs)));
+    n->s_rhs = nrhs;
+    return DWF_OK;
+}
+
+// Gaussian FP64 fields (n complex numbers) on the device.
+int lp_gauss(dwf_ctx* c, double2* out, long n, uint64_t seed)
+{
+    lp_gauss_kernel<<<grid_for(n, c->nsm), 256, 0, c->stream>>>(out, n, seed);
+    c->launches += 1;
+    CK(cudaGetLastError());
+    return DWF_OK;
+}
+
+}  // namespace
+
+void lp_destroy(dwf_ctx* c)
+{
+    LpNet* n = c->lp;
+    if (!n)
+        return;
+    void* bufs[] = {n->W, n->G, n->m, n->v, n->Bf, n->Ba, n->T, n->act[1], n->act[2], n->act[3],
+                    n->hid[0], n->hid[1], n->gbuf[0], n->gbuf[1], n->gpart, n->lpart, n->lscale,
+                    n->dloss, n->dconf, n->pr_rho, n->pr_e, n->s_r64, n->s_t64, n->s_rhs64,
+                    n->s_part2, n->s_part, n->s_val, n->s_state};
+    for (void* b : bufs)
+        if (b)
+            cudaFree(b);
+    for (float2* b : n->s_f32)
+        if (b)
+            cudaFree(b);
+    delete n;
+    c->lp = nullptr;
+}
+
+// Solve D x = src for nrhs sources: FP64 defect correction around an FP32
+// BiCGStab inner solve right-preconditioned by the network, then (for right-
+// hand sides that stall) the mixed CG on D^dag D from the current iterate.
+int lp_solve(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
+             double rtol, int maxiter, dwf_solve_info* info)
+{
+    LpNet* n = c->lp;
+    if (!n)
+        return ctx_fail(c, DWF_BAD_ARG, "learned solver: no network (dwf_lp_init first)");
+    if (nrhs < 1 || nrhs > 65535)
+        return ctx_fail(c, DWF_BAD_ARG, "learned solver: nrhs out of range");
+    const int* conf_d = nullptr;
+    ST(lp_conf(c, nrhs, conf_h, &conf_d));
+    ST(lp_transports(c));
+    ST(lp_ensure_solver(c, nrhs));
+    const long fs = c->fsz();
+    const long nf = fs * nrhs;
+    const int nblk = int(std::min<long>(64, (fs + 4095) / 4096));
+    float2 *r = n->s_f32[0], *rh = n->s_f32[1], *p = n->s_f32[2], *v = n->s_f32[3], *s = n->s_f32[4],
+           *t = n->s_f32[5], *ph = n->s_f32[6], *sh = n->s_f32[7], *x32 = n->s_f32[8];
+    double* val = n->s_val;  // [0] |r64|^2, [1] |D^dag r64|^2, [2] inverse norms, [3] scales
+    const dim3 rgrid(nblk, nrhs);
+    const int vgrid = grid_for(nf, c->nsm);
+    const int sgrid = (nrhs + 127) / 128;
+
+    // |D^dag src|^2 (stopping-rule denominator)
+    ST(apply_dev(c, DWF_OP_DDAG, nrhs, conf_d, 0, src, n->s_t64, 64));
+    lp_norm_kernel<<<rgrid, 256, 0, c->stream>>>(n->s_t64, fs, nblk, n->s_part);
+    lp_sum_kernel<<<sgrid, 128, 0, c->stream>>>(n->s_part, nrhs, nblk, val + 1);
+    c->launches += 2;
+    std::vector<double> bnorm2(nrhs), rnorm2(nrhs), nrm2(nrhs), prev(nrhs, -1.0), scale(nrhs);
+    CK(cudaMemcpyAsync(bnorm2.data(), val + 1, nrhs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemsetAsync(x, 0, size_t(nf) * sizeof(double2), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+
+    std::vector<int> done(nrhs, 0), stalled(nrhs, 0), iters(nrhs, 0), cycles(nrhs, 0);
+    std::vector<BsState> hs(nrhs);
+    std::vector<double> relres(nrhs, 1.0);
+    const double tgt2 = n->inner_tol * n->inner_tol;
+    long total_inner = 0;
+    for (int cyc = 0; cyc <= n->outer_max; ++cyc)
+    {
+        // r64 = src - D x; measure |D^dag r64| / |D^dag src|
+        ST(apply_dev(c, DWF_OP_D, nrhs, conf_d, 0, x, n->s_t64, 64));
+        lp_resid_kernel<<<rgrid, 256, 0, c->stream>>>(src, n->s_t64, n->s_r64, fs, nblk, n->s_part);
+        lp_sum_kernel<<<sgrid, 128, 0, c->stream>>>(n->s_part, nrhs, nblk, val);
+        ST(apply_dev(c, DWF_OP_DDAG, nrhs, conf_d, 0, n->s_r64, n->s_t64, 64));
+        lp_norm_kernel<<<rgrid, 256, 0, c->stream>>>(n->s_t64, fs, nblk, n->s_part);
+        lp_sum_kernel<<<sgrid, 128, 0, c->stream>>>(n->s_part, nrhs, nblk, val + nrhs);
+        c->launches += 4;
+        CK(cudaMemcpyAsync(rnorm2.data(), val, nrhs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(nrm2.data(), val + nrhs, nrhs * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        int left = 0;
+        for (int k = 0; k < nrhs; ++k)
+        {
+            relres[k] = bnorm2[k] > 0.0 ? std::sqrt(nrm2[k] / bnorm2[k]) : 0.0;
+            if (!std::isfinite(relres[k]))
+                stalled[k] = 1;
+            if (relres[k] <= rtol)
+                done[k] = 1;
+            // stall: the true residual fell by less than a factor 2 in a cycle
+            if (!done[k] && prev[k] >= 0.0 && relres[k] > 0.5 * prev[k])
+                stalled[k] = 1;
+            if (!done[k] && iters[k] >= maxiter)
+                stalled[k] = 1;
+            prev[k] = relres[k];
+            const bool go = !done[k] && !stalled[k];
+            left += go ? 1 : 0;
+            const double rn = std::sqrt(rnorm2[k]);
+            scale[k] = go && rn > 0.0 ? rn : 0.0;
+            hs[k].active = go ? 1 : 0;
+        }
+        if (!left || cyc == n->outer_max)
+            break;
+        // inner system D e = r64 / |r64| in FP32
+        std::vector<double> inv(nrhs);
+        for (int k = 0; k < nrhs; ++k)
+            inv[k] = scale[k] > 0.0 ? 1.0 / scale[k] : 0.0;
+        CK(cudaMemcpyAsync(val + 2 * nrhs, inv.data(), nrhs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(val + 3 * nrhs, scale.data(), nrhs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(n->s_state, hs.data(), nrhs * sizeof(BsState), cudaMemcpyHostToDevice, c->stream));
+        lp_down_kernel<<<vgrid, 256, 0, c->stream>>>(n->s_r64, val + 2 * nrhs, fs, nrhs, r);
+        CK(cudaMemcpyAsync(rh, r, size_t(nf) * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemsetAsync(p, 0, size_t(nf) * sizeof(float2), c->stream));
+        CK(cudaMemsetAsync(v, 0, size_t(nf) * sizeof(float2), c->stream));
+        CK(cudaMemsetAsync(x32, 0, size_t(nf) * sizeof(float2), c->stream));
+        lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, r}, Dot{r, r}, Dot{r, r}, 2, fs, nblk, n->s_part2);
+        lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(0, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+        c->launches += 3;
+        const int chunk = 4;
+        for (int it = 0; it < n->inner_max; it += chunk)
+        {
+            for (int u = 0; u < chunk; ++u)
+            {
+                if (it + u > 0)
+                {
+                    lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, r}, Dot{r, r}, Dot{r, r}, 2, fs, nblk, n->s_part2);
+                    lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(1, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+                    c->launches += 2;
+                }
+                else
+                {
+                    // first iteration: beta = 0, p = r
+                    lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(1, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+                    c->launches += 1;
+                }
+                lp_bs_vec_kernel<<<vgrid, 256, 0, c->stream>>>(0, fs, nrhs, n->s_state, p, r, v, s, x32, ph, sh, t, r);
+                ST(lp_net(c, false, nrhs, conf_d, p, ph, false));
+                ST(apply_dev(c, DWF_OP_D, nrhs, conf_d, 0, ph, v, 32));
+                lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, v}, Dot{rh, v}, Dot{rh, v}, 1, fs, nblk, n->s_part2);
+                lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(2, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+                lp_bs_vec_kernel<<<vgrid, 256, 0, c->stream>>>(1, fs, nrhs, n->s_state, p, r, v, s, x32, ph, sh, t, r);
+                ST(lp_net(c, false, nrhs, conf_d, s, sh, false));
+                ST(apply_dev(c, DWF_OP_D, nrhs, conf_d, 0, sh, t, 32));
+                lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{t, s}, Dot{t, t}, Dot{t, t}, 2, fs, nblk, n->s_part2);
+                lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(3, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+                lp_bs_vec_kernel<<<vgrid, 256, 0, c->stream>>>(2, fs, nrhs, n->s_state, p, r, v, s, x32, ph, sh, t, r);
+                c->launches += 7;
+            }
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(hs.data(), n->s_state, nrhs * sizeof(BsState), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            bool any = false;
+            for (int k = 0; k < nrhs; ++k)
+                any = any || hs[k].active;
+            if (!any)
+                break;
+        }
+        // the last coefficient step leaves rr of the final r; stop flags too
+        lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, r}, Dot{r, r}, Dot{r, r}, 2, fs, nblk, n->s_part2);
+        c->launches += 1;
+        CK(cudaMemcpyAsync(hs.data(), n->s_state, nrhs * sizeof(BsState), cudaMemcpyDeviceToHost, c->stream));
+        lp_up_kernel<<<vgrid, 256, 0, c->stream>>>(x, x32, val + 3 * nrhs, fs, nrhs);
+        c->launches += 1;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < nrhs; ++k)
+            if (scale[k] > 0.0)
+            {
+                iters[k] += hs[k].iters;
+                cycles[k] += 1;
+                total_inner += hs[k].iters;
+            }
+    }
+    n->iters_total += total_inner;
+    // fallback: mixed CG on D^dag D from the current iterate
+    std::vector<int> fb(nrhs, 0);
+    int nfb = 0;
+    for (int k = 0; k < nrhs; ++k)
+        if (!done[k])
+        {
+            fb[k] = 1;
+            ++nfb;
+        }
+    std::vector<dwf_solve_info> fbi(nrhs);
+    if (nfb)
+    {
+        ST(apply_dev(c, DWF_OP_DDAG, nrhs, conf_d, 0, src, n->s_rhs64, 64));
+        ST(solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, n->s_rhs64, x, 1, rtol, maxiter,
+                       DWF_SOLVER_MIXED, 0, fbi.data()));
+    }
+    else
+    {
+        // every right-hand side met the rule on the FP64 true residual above
+        for (int k = 0; k < nrhs; ++k)
+            fbi[k].true_relres = relres[k];
+    }
+    for (int k = 0; info && k < nrhs; ++k)
+    {
+        dwf_solve_info& I = info[k];
+        I.iterations = iters[k] + (fb[k] ? fbi[k].iterations : 0);
+        I.true_relres = fbi[k].true_relres;
+        I.relres = fb[k] ? fbi[k].relres : relres[k];
+        I.status = fb[k] ? fbi[k].status : DWF_OK;
+        if (I.status == DWF_OK && !(I.true_relres <= rtol))
+            I.status = std::isfinite(I.true_relres) ? DWF_NOT_CONVERGED : DWF_NONFINITE;
+        I.converged = I.status == DWF_OK ? 1 : 0;
+        I.solver = DWF_SOLVER_LEARNED;
+        I.reliable_updates = cycles[k];
+        I.fallback = fb[k];
+        I.dirac_relres = 0.0;
+        I.schur_iterations = iters[k];  // preconditioned iterations (2 network + 2 D each)
+    }
+    return DWF_OK;
+}
+
+}  // namespace dwfb
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int dwf_lp_init(dwf_ctx* c, int hidden, uint64_t seed)
+{
+    if (!c)
+        return DWF_BAD_ARG;
+    if (hidden != 8 && hidden != 16 && hidden != 32)
+        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: hidden must be 8, 16 or 32");
+    const int C0 = 2 * c->L.Ls;
+    if (C0 > 48 || C0 * hidden > kGradThreads * kGradMaxPer)
+        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: 2*Ls*hidden must be <= 1024 and Ls <= 24");
+    CK(cudaSetDevice(c->device));
+    lp_destroy(c);
+    LpNet* n = new LpNet();
+    c->lp = n;
+    n->C0 = C0;
+    n->H = hidden;
+    const int ch[kLpLayers + 1] = {C0, hidden, hidden, hidden, C0};
+    n->woff[0] = n->bf_off[0] = n->ba_off[0] = 0;
+    for (int l = 0; l < kLpLayers; ++l)
+    {
+        n->cin[l] = ch[l];
+        n->cout[l] = ch[l + 1];
+        n->ksteps[l] = (9 * ch[l] + 7) / 8;
+        n->ntf[l] = nt_of(ch[l + 1]);
+        n->nta[l] = nt_of(ch[l]);
+        n->woff[l + 1] = n->woff[l] + 9L * ch[l] * ch[l + 1];
+        n->bf_off[l + 1] = n->bf_off[l] + long(n->ksteps[l]) * n->ntf[l] * 32;
+        n->ba_off[l + 1] = n->ba_off[l] + long((9 * ch[l + 1] + 7) / 8) * n->nta[l] * 32;
+    }
+    const long nw = n->woff[kLpLayers];
+    ST(lp_grow(c, n->W, nw));
+    ST(lp_grow(c, n->G, nw));
+    ST(lp_grow(c, n->m, 2 * nw));
+    ST(lp_grow(c, n->v, 2 * nw));
+    ST(lp_grow(c, n->Bf, n->bf_off[kLpLayers]));
+    ST(lp_grow(c, n->Ba, n->ba_off[kLpLayers]));
+    CK(cudaMemsetAsync(n->m, 0, 2 * nw * sizeof(float), c->stream));
+    CK(cudaMemsetAsync(n->v, 0, 2 * nw * sizeof(float), c->stream));
+    // initial weights: small seeded Gaussian noise, plus the identity on the
+    // centre offset of each layer (scaled 1/2 in the first), so that N starts
+    // close to a multiple of the identity on the channels every layer keeps
+    std::mt19937_64 gen(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    std::vector<float2> w(nw);
+    for (int l = 0; l < kLpLayers; ++l)
+    {
+        const double sd = 0.02 / std::sqrt(9.0 * n->cin[l]);
+        for (long i = n->woff[l]; i < n->woff[l + 1]; ++i)
+        {
+            const double re = nd(gen) * sd;
+            const double im = nd(gen) * sd;
+            w[i] = make_float2(float(re), float(im));
+        }
+        for (int o = 0; o < std::min(n->cin[l], n->cout[l]); ++o)
+            w[n->woff[l] + long(o) * n->cin[l] + o].x += (l == 0) ? 0.5f : 1.0f;
+    }
+    CK(cudaMemcpyAsync(n->W, w.data(), nw * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    ST(lp_pack(c));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+int dwf_lp_weights_size(const dwf_ctx* c, long* n_complex)
+{
+    if (!c || !c->lp || !n_complex)
+        return DWF_BAD_ARG;
+    *n_complex = c->lp->woff[kLpLayers];
+    return DWF_OK;
+}
+
+int dwf_lp_get_weights(dwf_ctx* c, float* w)
+{
+    if (!c || !c->lp || !w)
+        return DWF_BAD_ARG;
+    CK(cudaMemcpyAsync(w, c->lp->W, c->lp->woff[kLpLayers] * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+int dwf_lp_set_weights(dwf_ctx* c, const float* w)
+{
+    if (!c || !c->lp || !w)
+        return DWF_BAD_ARG;
+    CK(cudaMemcpyAsync(c->lp->W, w, c->lp->woff[kLpLayers] * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    c->lp->adam_t = 0;
+    CK(cudaMemsetAsync(c->lp->m, 0, 2 * c->lp->woff[kLpLayers] * sizeof(float), c->stream));
+    CK(cudaMemsetAsync(c->lp->v, 0, 2 * c->lp->woff[kLpLayers] * sizeof(float), c->stream));
+    ST(lp_pack(c));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+int dwf_lp_transports(dwf_ctx* c, int conf, float* T)
+{
+    if (!c || !c->lp || !T || conf < 0 || conf >= c->nconf)
+        return DWF_BAD_ARG;
+    ST(lp_transports(c));
+    CK(cudaMemcpyAsync(T, c->lp->T + long(conf) * c->L.V * 9, size_t(c->L.V) * 9 * sizeof(float2),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DWF_OK;
+}
+
+int dwf_lp_apply_dev(dwf_ctx* c, int adjoint, int nrhs, const int* rhs_conf, const void* in, void* out)
+{
+    if (!c || !c->lp || !in || !out || nrhs < 1 || nrhs > 65535)
+        return c ? ctx_fail(c, DWF_BAD_ARG, "dwf_lp_apply_dev: bad arguments or no network") : DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    const int* conf_d = nullptr;
+    ST(lp_conf(c, nrhs, rhs_conf, &conf_d));
+    ST(lp_transports(c));
+    ST(lp_net(c, adjoint != 0, nrhs, conf_d, static_cast<const float2*>(in), static_cast<float2*>(out), false));
+    return DWF_OK;
+}
+
+int dwf_lp_layer_dev(dwf_ctx* c, int layer, int adjoint, int nrhs, const int* rhs_conf, const void* in,
+                     void* out)
+{
+    if (!c || !c->lp || !in || !out || nrhs < 1 || nrhs > 65535 || layer < 0 || layer >= kLpLayers)
+        return c ? ctx_fail(c, DWF_BAD_ARG, "dwf_lp_layer_dev: bad arguments or no network") : DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    const int* conf_d = nullptr;
+    ST(lp_conf(c, nrhs, rhs_conf, &conf_d));
+    ST(lp_transports(c));
+    LpNet* n = c->lp;
+    const int ci = adjoint ? n->cout[layer] : n->cin[layer];
+    const int co = adjoint ? n->cin[layer] : n->cout[layer];
+    ST(lp_layer(c, layer, adjoint != 0, nrhs, conf_d, static_cast<const float2*>(in), net_layout(c, ci),
+                static_cast<float2*>(out), net_layout(c, co)));
+    return DWF_OK;
+}
+
+int dwf_lp_loss_grad_dev(dwf_ctx* c, int npair, const int* pair_conf, const void* rho, const void* e,
+                         double* loss, float* grad)
+{
+    if (!c || !c->lp || !rho || !e || npair < 1 || npair > 1024)
+        return c ? ctx_fail(c, DWF_BAD_ARG, "dwf_lp_loss_grad_dev: bad arguments or no network") : DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    const int* conf_d = nullptr;
+    ST(lp_conf(c, npair, pair_conf, &conf_d));
+    ST(lp_transports(c));
+    ST(lp_loss_grad(c, npair, conf_d, static_cast<const float2*>(rho), static_cast<const float2*>(e), loss));
+    if (grad)
+    {
+        CK(cudaMemcpyAsync(grad, c->lp->G, c->lp->woff[kLpLayers] * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return DWF_OK;
+}
+
+// Training pairs: for each configuration, `pairs_per_conf` pairs. A fraction
+// come from the plain solver (error of a truncated CG iterate against the
+// converged solution, rho = D e); the rest are e ~ Gaussian, rho = D e.
+int dwf_lp_train(dwf_ctx* c, const dwf_lp_train_params* tp, dwf_lp_train_info* ti, double* history)
+{
+    if (!c || !c->lp || !tp || tp->steps < 0 || tp->batch < 1 || tp->batch > 1024 ||
+        tp->pairs_per_conf < 1 || !(tp->lr > 0.0))
+        return c ? ctx_fail(c, DWF_BAD_ARG, "dwf_lp_train: bad parameters or no network") : DWF_BAD_ARG;
+    if (c->nconf < 1)
+        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_train: no gauge configuration (set_gauge first)");
+    CK(cudaSetDevice(c->device));
+    LpNet* n = c->lp;
+    const auto t0 = std::chrono::steady_clock::now();
+    ST(lp_transports(c));
+    const long fs = c->fsz();
+    const int np = c->nconf * tp->pairs_per_conf;
+    if (np != n->npairs)
+    {
+        ST(lp_grow(c, n->pr_rho, size_t(np) * fs));
+        ST(lp_grow(c, n->pr_e, size_t(np) * fs));
+        n->npairs = np;
+    }
+    n->pr_conf.assign(np, 0);
+    for (int k = 0; k < np; ++k)
+        n->pr_conf[k] = k / tp->pairs_per_conf;
+    // generate pairs in groups of up to 16 (FP64 staging in the solver
+    // workspace); group g is a solver group when g % solver_every == 0
+    const int grp = std::min(np, 16);
+    ST(lp_ensure_solver(c, grp));
+    int nsolver = 0;
+    const int* conf_d = nullptr;
+    for (int k0 = 0; k0 < np; k0 += grp)
+    {
+        const int m = std::min(grp, np - k0);
+        ST(lp_conf(c, m, n->pr_conf.data() + k0, &conf_d));
+        const bool solver_pair = tp->solver_iters > 0 &&
+                                 (k0 / grp) % std::max(1, tp->solver_every) == 0;
+        ST(lp_gauss(c, n->s_r64, long(m) * fs, tp->seed * 0x100000001B3ull + uint64_t(k0)));
+        if (solver_pair)
+        {
+            // b Gaussian; x* = converged CG solution of D^dag D x = D^dag b;
+            // x_k = CG truncated at solver_iters; e = x* - x_k
+            std::vector<int> cf(n->pr_conf.begin() + k0, n->pr_conf.begin() + k0 + m);
+            ST(apply_dev(c, DWF_OP_DDAG, m, conf_d, 0, n->s_r64, n->s_rhs64, 64));
+            std::vector<dwf_solve_info> inf(m);
+            ST(solve_batch(c, DWF_OP_DDAGD, m, cf.data(), n->s_rhs64, n->s_t64, 0, 1e-8,
+                           std::max(tp->solver_maxiter, 1), DWF_SOLVER_MIXED, 0, inf.data()));
+            ST(solve_batch(c, DWF_OP_DDAGD, m, cf.data(), n->s_rhs64, n->s_r64, 0, 1e-30,
+                           tp->solver_iters, DWF_SOLVER_CG64, 0, inf.data()));
+            lp_diff_kernel<<<grid_for(long(m) * fs, c->nsm), 256, 0, c->stream>>>(
+                n->s_t64, n->s_r64, n->pr_e + long(k0) * fs, long(m) * fs);
+            nsolver += m;
+        }
+        else
+            lp_f64_to_f32_kernel<<<grid_for(long(m) * fs, c->nsm), 256, 0, c->stream>>>(
+                n->s_r64, n->pr_e + long(k0) * fs, long(m) * fs);
+        c->launches += 1;
+        CK(cudaGetLastError());
+        ST(apply_dev(c, DWF_OP_D, m, conf_d, 0, n->pr_e + long(k0) * fs, n->pr_rho + long(k0) * fs, 32));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    const auto t1 = std::chrono::steady_clock::now();
+    // Adam over mini-batches drawn in a seeded shuffled order
+    std::mt19937_64 gen(tp->seed ^ 0x5DEECE66Dull);
+    std::vector<int> order(np);
+    for (int k = 0; k < np; ++k)
+        order[k] = k;
+    const int B = std::min(tp->batch, np);
+    ST(lp_ensure_act(c, B));
+    float2* brho = nullptr;
+    float2* be = nullptr;
+    CK(cudaMalloc(&brho, size_t(B) * fs * sizeof(float2)));
+    CK(cudaMalloc(&be, size_t(B) * fs * sizeof(float2)));
+    double first = -1.0, last = -1.0;
+    int pos = np;
+    std::vector<int> bc(B);
+    int st = DWF_OK;
+    for (int step = 0; step < tp->steps && st == DWF_OK; ++step)
+    {
+        if (pos + B > np)
+        {
+            std::shuffle(order.begin(), order.end(), gen);
+            pos = 0;
+        }
+        for (int b = 0; b < B; ++b)
+        {
+            const int k = order[pos + b];
+            bc[b] = n->pr_conf[k];
+            cudaMemcpyAsync(brho + long(b) * fs, n->pr_rho + long(k) * fs, fs * sizeof(float2),
+                            cudaMemcpyDeviceToDevice, c->stream);
+            cudaMemcpyAsync(be + long(b) * fs, n->pr_e + long(k) * fs, fs * sizeof(float2),
+                            cudaMemcpyDeviceToDevice, c->stream);
+        }
+        pos += B;
+        st = lp_conf(c, B, bc.data(), &conf_d);
+        const bool logit = history || step == 0 || step == tp->steps - 1;
+        double L = 0.0;
+        if (st == DWF_OK)
+            st = lp_loss_grad(c, B, conf_d, brho, be, logit ? &L : nullptr);
+        if (st == DWF_OK)
+        {
+            const double lr = tp->lr * (tp->lr_decay_steps > 0 ? std::pow(0.5, double(step) / tp->lr_decay_steps) : 1.0);
+            st = lp_adam(c, lr);
+        }
+        if (logit)
+        {
+            if (first < 0.0)
+                first = L;
+            last = L;
+            if (history)
+                history[step] = L;
+        }
+    }
+    cudaStreamSynchronize(c->stream);
+    cudaFree(brho);
+    cudaFree(be);
+    if (st != DWF_OK)
+        return st;
+    const auto t2 = std::chrono::steady_clock::now();
+    if (ti)
+    {
+        ti->loss_first = first;
+        ti->loss_last = last;
+        ti->steps = tp->steps;
+        ti->npairs = np;
+        ti->solver_pairs = nsolver;
+        ti->seconds_pairs = std::chrono::duration<double>(t1 - t0).count();
+        ti->seconds_train = std::chrono::duration<double>(t2 - t1).count();
+    }
+    return DWF_OK;
+}
+
+int dwf_lp_set_solver(dwf_ctx* c, double inner_tol, int inner_maxiter, int outer_max)
+{
+    if (!c || !c->lp || !(inner_tol > 0.0 && inner_tol < 1.0) || inner_maxiter < 1 || outer_max < 1)
+        return c ? ctx_fail(c, DWF_BAD_ARG, "dwf_lp_set_solver: bad arguments or no network") : DWF_BAD_ARG;
+    c->lp->inner_tol = inner_tol;
+    c->lp->inner_max = inner_maxiter;
+    c->lp->outer_max = outer_max;
+    return DWF_OK;
+}
+
+}  // extern "C"

@@ -16,6 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _capi as A
+from .learned import LearnedMixin
 
 
 @dataclass
@@ -31,7 +32,7 @@ def _ptr(a):
     return C.c_void_p(a.ctypes.data)
 
 
-class DomainWall:
+class DomainWall(LearnedMixin):
     """One device context for a domain-wall lattice (dwf.Nt, dwf.Nx, dwf.N5,
     dwf.M5, dwf.mf, dwf.beta)."""
 

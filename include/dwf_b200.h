@@ -409,6 +409,10 @@ typedef struct
  * of every step. */
 int dwf_lp_train(dwf_ctx* ctx, const dwf_lp_train_params* params, dwf_lp_train_info* info,
                  double* history);
+/* Layer kernel: -1 automatic (default: the tcgen05 kernel wherever its shared-
+ * memory tile fits, else the mma.sync kernel), 0 the mma.sync kernel, 1 the
+ * tcgen05 kernel only (DWF_BAD_ARG where it does not fit). */
+int dwf_lp_set_variant(dwf_ctx* ctx, int variant);
 /* Inner solve: stop at |r| <= inner_tol |r0| or inner_maxiter iterations;
  * at most outer_max defect-correction cycles (defaults 1e-4, 400, 40). */
 int dwf_lp_set_solver(dwf_ctx* ctx, double inner_tol, int inner_maxiter, int outer_max);

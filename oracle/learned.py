@@ -13,11 +13,13 @@ arithmetic in numpy so that the GPU kernels can be checked against it:
 * the network is four such layers, C0 -> H -> H -> H -> C0, without bias or
   activation, so it is linear and gauge covariant, and its adjoint is the
   same chain run backwards with W'_k = (W_rev(k))^H;
-* the GPU computes the transported values a in FP32 without fused
-  multiply-add, rounds them and the weights to BF16 (round to nearest even)
-  and accumulates in FP32 on the tensor cores; ``rounded=True`` reproduces the
-  rounding exactly and accumulates in FP64, ``rounded=False`` is the exact
-  FP64 network used for the finite-difference gradient checks.
+* the GPU evaluates a layer as out(y) = sum_k T_k(y) P_k(y + d_k) with
+  P_k = W_k in: the input field and the weights are rounded to BF16 (round to
+  nearest even), P_k is accumulated in FP32 on the tensor cores, and the
+  transporter products and the sum over k are FP32; ``rounded=True``
+  reproduces the rounding of the operands exactly and accumulates in FP64,
+  ``rounded=False`` is the exact FP64 network used for the finite-difference
+  gradient checks.
 
 Fields enter and leave in the operator's own layout (domain wall: index
 ((s*Nt+t)*Nx+x)*2+spin, channel c = 2*s+spin; Wilson: (t*Nx+x)*2+spin,
@@ -86,17 +88,6 @@ def bf16c(z):
         1j * bf16(z.imag.astype(np.float32)).astype(np.float64)
 
 
-def tmul32(T, v):
-    """Complex product T*v in float32, each multiply and add rounded (no FMA)."""
-    tr = T.real.astype(np.float32)
-    ti = T.imag.astype(np.float32)
-    vr = v.real.astype(np.float32)
-    vi = v.imag.astype(np.float32)
-    re = (tr * vr).astype(np.float32) - (ti * vi).astype(np.float32)
-    im = (tr * vi).astype(np.float32) + (ti * vr).astype(np.float32)
-    return re.astype(np.float64) + 1j * im.astype(np.float64)
-
-
 def to_net(f, V, C):
     """Operator layout (flat, per right-hand side) -> [B, V, C]."""
     f = np.asarray(f).reshape(-1, C // 2, V, 2)
@@ -110,11 +101,12 @@ def from_net(g, V, C):
 
 
 def gather(T, nb, fin, k, rounded):
-    """a_k = T_k * fin(neighbour k) for fin [B, V, Cin]."""
+    """a_k = T_k * fin(neighbour k) for fin [B, V, Cin] (fin rounded to BF16
+    when rounded)."""
     v = fin[:, nb[:, k], :]
     t = T[:, k][None, :, None]
     if rounded:
-        return bf16c(tmul32(t.astype(np.complex64), v.astype(np.complex64)))
+        return t * bf16c(v)
     return t * v
 
 

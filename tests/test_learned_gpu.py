@@ -50,9 +50,12 @@ def test_transports_match_oracle(T):
     d.close()
 
 
+@pytest.mark.parametrize("variant", [1, 0])
 @pytest.mark.parametrize("adjoint", [False, True])
-def test_each_layer_matches_oracle(T, torch, adjoint):
+def test_each_layer_matches_oracle(T, torch, adjoint, variant):
+    """Both layer kernels (1: tcgen05 with TMEM accumulators, 0: mma.sync)."""
     d, th, ws = setup_dwf(T)
+    d.lp_set_variant(variant)
     rng = np.random.default_rng(11)
     V = d.Nt * d.Nx
     nb = LN.neighbours(d.Nt, d.Nx)
@@ -73,8 +76,10 @@ def test_each_layer_matches_oracle(T, torch, adjoint):
     d.close()
 
 
-def test_network_matches_oracle(T, torch):
+@pytest.mark.parametrize("variant", [1, 0])
+def test_network_matches_oracle(T, torch, variant):
     d, th, ws = setup_dwf(T)
+    d.lp_set_variant(variant)
     rng = np.random.default_rng(12)
     V, C0 = d.Nt * d.Nx, 2 * d.Ls
     nb = LN.neighbours(d.Nt, d.Nx)
@@ -100,8 +105,10 @@ def test_network_matches_oracle(T, torch):
     d.close()
 
 
-def test_loss_and_gradient_match_oracle(T, torch):
+@pytest.mark.parametrize("variant", [1, 0])
+def test_loss_and_gradient_match_oracle(T, torch, variant):
     d, th, ws = setup_dwf(T)
+    d.lp_set_variant(variant)
     rng = np.random.default_rng(13)
     V, C0 = d.Nt * d.Nx, 2 * d.Ls
     nb = LN.neighbours(d.Nt, d.Nx)
@@ -119,6 +126,24 @@ def test_loss_and_gradient_match_oracle(T, torch):
     _, gx = LN.loss_grad(Tg, nb, ws, LN.to_net(rho, V, C0), LN.to_net(e, V, C0), rounded=False)
     for l in range(4):
         assert rel(grads[l], gx[l]) < 5e-2, l
+    d.close()
+
+
+def test_layer_variants_agree_at_width_32(T, torch):
+    """tcgen05 and mma.sync layers on a 32-channel domain-wall field (Ls = 16,
+    hidden 32: the widths of the benchmark) agree to FP32 accumulation order."""
+    rng = np.random.default_rng(17)
+    d = T.DomainWall(16, 64, 16, 1.0, 0.05)
+    d.set_gauge(quenched_theta(rng, 16, 64, 3.0)[None])
+    d.lp_init(hidden=32, seed=2)
+    f = torch.from_numpy(crand(rng, 3, d.Ndof)).cuda()
+    outs = []
+    for v in (1, 0):
+        d.lp_set_variant(v)
+        o = torch.empty_like(f)
+        d.lp_apply_dev(f, o)
+        outs.append(o.cpu().numpy())
+    assert rel(outs[0], outs[1]) < 1e-3
     d.close()
 
 

@@ -134,6 +134,7 @@ SIGNATURES = {
     "dwf_lp_loss_grad_dev": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double), _P]),
     "dwf_lp_train": (_I, [_P, C.POINTER(LpTrainParams), C.POINTER(LpTrainInfo), _P]),
     "dwf_lp_set_solver": (_I, [_P, _D, _I, _I]),
+    "dwf_lp_set_variant": (_I, [_P, _I]),
 }
 
 _lib = None

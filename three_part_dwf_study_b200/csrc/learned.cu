@@ -131,12 +131,14 @@ __global__ void lp_transport_kernel(Lat L, const double2* __restrict__ U64, long
 // ---------------------------------------------------------------------------
 // weight packing into mma.m16n8k16 B fragments
 // ---------------------------------------------------------------------------
-// The complex contraction out[o] = sum_j W[o][j] a[j] is the real product of
+// The complex contraction P[o] = sum_j W[o][j] a[j] is the real product of
 // A = [re a_j, im a_j]_j (interleaved) with B[2j][2o] = Re W, B[2j+1][2o] = -Im W,
-// B[2j][2o+1] = Im W, B[2j+1][2o+1] = Re W. Fragment of lane (g = lane/4,
+// B[2j][2o+1] = Im W, B[2j+1][2o+1] = Re W. Input channels are padded to
+// cpad (a multiple of 8) per offset; k-step ks covers offset k = ks / (cpad/8)
+// and channels 8 (ks % (cpad/8)) .. +7. Fragment of lane (g = lane/4,
 // q = lane%4) for k-step ks and n-tile nt: real column n = 8 nt + g (output
-// o = n/2, part n%2), rows of activations j = 8 ks + q (b0) and j + 4 (b1),
-// low half the row of Re a_j.
+// o = n/2, part n%2), activation rows j = 8 ks + q (b0) and j + 4 (b1), the
+// low half holding the row of Re a_j.
 __device__ __forceinline__ uint32_t pack_bf2(float lo, float hi)
 {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -144,11 +146,12 @@ __device__ __forceinline__ uint32_t pack_bf2(float lo, float hi)
 }
 
 __global__ void lp_pack_kernel(const float2* __restrict__ W, int cin, int cout, int adjoint,
-                               int ksteps, int nt, uint2* __restrict__ B)
+                               int cpad, int nt, uint2* __restrict__ B)
 {
     // layer dimensions as seen by the packed (possibly adjoint) layer
     const int ci = adjoint ? cout : cin;
     const int co = adjoint ? cin : cout;
+    const int ksteps = 9 * cpad / 8;
     const int total = ksteps * nt * 32;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x)
     {
@@ -162,10 +165,10 @@ __global__ void lp_pack_kernel(const float2* __restrict__ W, int cin, int cout, 
         for (int h = 0; h < 2; ++h)
         {
             const int j = 8 * ks + q + 4 * h;
+            const int k = j / cpad, i = j - k * cpad;
             float2 w = make_float2(0.f, 0.f);
-            if (o < co && j < 9 * ci)
+            if (o < co && i < ci)
             {
-                const int k = j / ci, i = j - k * ci;
                 if (!adjoint)
                     w = W[(long(k) * cout + o) * cin + i];
                 else
@@ -183,22 +186,32 @@ __global__ void lp_pack_kernel(const float2* __restrict__ W, int cin, int cout, 
 }
 
 // ---------------------------------------------------------------------------
-// PTC layer on the tensor cores
+// PTC layer as an implicit GEMM on the tensor cores
 // ---------------------------------------------------------------------------
-struct PtcArgs
+// out(y) = sum_k T_k(y) P_k(y + d_k), P_k = W_k in. A block owns a tile of
+// kTileRows t-rows x tx x-sites of one right-hand side: it stages the input
+// on the tile and its one-site halo in shared memory as BF16 (site-major,
+// channels padded to cpad with a 4-word skew so ldmatrix rows hit distinct
+// banks); each warp then computes 16 consecutive x-sites: per offset k the
+// A fragments of the shifted window come from ldmatrix, the B fragments
+// (weights) from shared memory, P_k accumulates in FP32 registers and is
+// multiplied by the FP32 transporter of each row before it joins the sum.
+struct ConvArgs
 {
     const float2* in;
     float2* out;
     FieldLayout li, lo;
-    int cin, cout, ksteps;
-    const uint2* B;
-    const float2* T;
+    int cin, cout, cpad;   // channels; input channels padded to a multiple of 8
+    int tx;                // tile width in x (multiple of 16)
+    const uint2* B;        // [9 * cpad / 8][NT][32]
+    const float2* T;       // [nconf][V][9]
     const int* conf;
     int conf0;
     int Nt, Nx, V, nrhs;
 };
 
-constexpr int kPtcWarps = 4;
+constexpr int kConvWarps = 8;
+constexpr int kTileRows = 2;
 
 __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
                                          uint32_t a3, uint32_t b0, uint32_t b1)
@@ -210,121 +223,742 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// bf16 pair of T * v, the complex product rounded per operation (no FMA), so
-// that the rounding to BF16 sees exactly the FP32 value the oracle computes.
-__device__ __forceinline__ uint32_t transported(float2 T, float2 v)
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void* p)
 {
-    const float re = __fsub_rn(__fmul_rn(T.x, v.x), __fmul_rn(T.y, v.y));
-    const float im = __fadd_rn(__fmul_rn(T.x, v.y), __fmul_rn(T.y, v.x));
-    return pack_bf2(re, im);
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
 }
 
-__host__ __device__ __forceinline__ size_t ptc_smem_bytes(int ksteps, int nt)
+__host__ __device__ __forceinline__ int conv_site_words(int cpad) { return cpad + 4; }
+
+__host__ __device__ __forceinline__ size_t conv_smem_bytes(int cpad, int nt, int tx)
 {
-    return size_t(ksteps) * nt * 32 * sizeof(uint2) + size_t(16) * ksteps * sizeof(int) +
-           size_t(kPtcWarps) * 144 * (sizeof(int) + sizeof(float2));
+    return size_t(9) * (cpad / 8) * nt * 32 * sizeof(uint2) +
+           size_t(kTileRows + 2) * (tx + 2) * conv_site_words(cpad) * sizeof(uint32_t);
 }
 
-// One warp computes 16 sites x all output channels of one right-hand side per
-// tile: A fragments are gathered straight from global memory (neighbour
-// value times transporter, rounded to BF16), B fragments come from shared memory.
 template <int NT>
-__global__ void __launch_bounds__(kPtcWarps * 32) lp_ptc_kernel(PtcArgs a)
+__global__ void __launch_bounds__(kConvWarps * 32) lp_conv_kernel(ConvArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2* Bs = reinterpret_cast<uint2*>(smem);
-    const int nb_frag = a.ksteps * NT * 32;
-    float2* Tsh = reinterpret_cast<float2*>(Bs + nb_frag);        // [warps][144]
-    int* kd = reinterpret_cast<int*>(Tsh + kPtcWarps * 144);     // [8 ksteps]
-    int* co = kd + 8 * a.ksteps;                                  // [8 ksteps]
-    int* nbs = co + 8 * a.ksteps;                                 // [warps][144]
+    const int ks_per = a.cpad / 8;
+    const int nb_frag = 9 * ks_per * NT * 32;
+    uint32_t* tile = reinterpret_cast<uint32_t*>(Bs + nb_frag);
+    const int SW = conv_site_words(a.cpad);
+    const int TW = a.tx + 2;
     for (int i = threadIdx.x; i < nb_frag; i += blockDim.x)
         Bs[i] = a.B[i];
-    for (int j = threadIdx.x; j < 8 * a.ksteps; j += blockDim.x)
-    {
-        if (j < 9 * a.cin)
-        {
-            const int k = j / a.cin, c = j - k * a.cin;
-            kd[j] = k;
-            co[j] = int(chan_off(a.li, c));
-        }
-        else
-        {
-            kd[j] = 0;  // padding: any finite value, its weights are zero
-            co[j] = 0;
-        }
-    }
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
-    float2* wT = Tsh + warp * 144;
-    int* wnb = nbs + warp * 144;
-    const int tiles_per_rhs = (a.V + 15) / 16;
-    const long ntiles = long(tiles_per_rhs) * a.nrhs;
-    for (long tile = long(blockIdx.x) * kPtcWarps + warp; tile < ntiles;
-         tile += long(gridDim.x) * kPtcWarps)
+    const int rows_t = (a.Nt + kTileRows - 1) / kTileRows;
+    const int cols_t = (a.Nx + a.tx - 1) / a.tx;
+    const long ntiles = long(rows_t) * cols_t * a.nrhs;
+    const int npairs = a.cpad / 2;  // channel pairs per site
+    const int mt_per_row = a.tx / 16;
+    for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x)
     {
-        const int rhs = int(tile / tiles_per_rhs);
-        const int h0 = int(tile - long(rhs) * tiles_per_rhs) * 16;
+        const int rhs = int(tl / (long(rows_t) * cols_t));
+        const int rem = int(tl - long(rhs) * rows_t * cols_t);
+        const int t0 = (rem / cols_t) * kTileRows;
+        const int x0 = (rem - (rem / cols_t) * cols_t) * a.tx;
         const int cf = a.conf ? a.conf[rhs] : a.conf0;
-        const float2* Tc = a.T + long(cf) * a.V * 9;
-        __syncwarp();
-        for (int e = lane; e < 144; e += 32)
-        {
-            const int r = e / 9, k = e - 9 * (e / 9);
-            const int h = h0 + r;
-            if (h < a.V)
-            {
-                const int t = h / a.Nx, x = h - t * a.Nx;
-                int tt = t + kOffT[k], xx = x + kOffX[k];
-                tt = tt < 0 ? tt + a.Nt : (tt >= a.Nt ? tt - a.Nt : tt);
-                xx = xx < 0 ? xx + a.Nx : (xx >= a.Nx ? xx - a.Nx : xx);
-                wnb[e] = (tt * a.Nx + xx) * a.li.hs;
-                wT[e] = Tc[long(h) * 9 + k];
-            }
-            else
-            {
-                wnb[e] = 0;
-                wT[e] = make_float2(0.f, 0.f);
-            }
-        }
-        __syncwarp();
         const float2* inr = a.in + long(rhs) * a.li.rs;
-        float acc[NT][4];
-#pragma unroll
-        for (int n = 0; n < NT; ++n)
-            acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
-        const int e0 = g * 9, e1 = (g + 8) * 9;
-        for (int ks = 0; ks < a.ksteps; ++ks)
+        __syncthreads();  // previous tile's readers are done
+        // stage the input on the tile and its halo (2 channels per thread step)
+        const int nstage = (kTileRows + 2) * TW * npairs;
+        for (int e = threadIdx.x; e < nstage; e += blockDim.x)
         {
-            const int j0 = 8 * ks + q, j1 = j0 + 4;
-            const int k0 = kd[j0], c0 = co[j0], k1 = kd[j1], c1 = co[j1];
-            const uint32_t A0 = transported(wT[e0 + k0], inr[wnb[e0 + k0] + c0]);
-            const uint32_t A1 = transported(wT[e1 + k0], inr[wnb[e1 + k0] + c0]);
-            const uint32_t A2 = transported(wT[e0 + k1], inr[wnb[e0 + k1] + c1]);
-            const uint32_t A3 = transported(wT[e1 + k1], inr[wnb[e1 + k1] + c1]);
-            const uint2* bp = Bs + ks * NT * 32 + lane;
+            const int site = e / npairs, cp = e - site * npairs;
+            const int r = site / TW, cc = site - r * TW;
+            int t = t0 - 1 + r, x = x0 - 1 + cc;
+            t = t < 0 ? t + a.Nt : (t >= a.Nt ? t - a.Nt : t);
+            x = x % a.Nx;  // x0 - 1 + cc >= -1
+            x = x < 0 ? x + a.Nx : x;
+            const int h = t * a.Nx + x;
+            uint32_t w0 = 0u, w1 = 0u;
+            const int c0 = 2 * cp;
+            if (c0 < a.cin)
+            {
+                if (c0 + 1 < a.cin && chan_off(a.li, c0 + 1) == chan_off(a.li, c0) + 1)
+                {
+                    const float4 v = *reinterpret_cast<const float4*>(inr + long(h) * a.li.hs + chan_off(a.li, c0));
+                    w0 = pack_bf2(v.x, v.y);
+                    w1 = pack_bf2(v.z, v.w);
+                }
+                else
+                {
+                    const float2 v = inr[long(h) * a.li.hs + chan_off(a.li, c0)];
+                    w0 = pack_bf2(v.x, v.y);
+                    if (c0 + 1 < a.cin)
+                    {
+                        const float2 u = inr[long(h) * a.li.hs + chan_off(a.li, c0 + 1)];
+                        w1 = pack_bf2(u.x, u.y);
+                    }
+                }
+            }
+            uint32_t* d = tile + site * SW + c0;
+            d[0] = w0;
+            d[1] = w1;
+        }
+        __syncthreads();
+        const float2* Tc = a.T + long(cf) * a.V * 9;
+        float2* outr = a.out + long(rhs) * a.lo.rs;
+        for (int mt = warp; mt < kTileRows * mt_per_row; mt += kConvWarps)
+        {
+            const int r = mt / mt_per_row;
+            const int xs = (mt - r * mt_per_row) * 16;
+            const int t = t0 + r;
+            const bool row_ok = t < a.Nt;
+            const int xg0 = x0 + xs + g, xg1 = xg0 + 8;
+            const bool ok0 = row_ok && xg0 < a.Nx, ok1 = row_ok && xg1 < a.Nx;
+            const int h0 = t * a.Nx + xg0, h1 = t * a.Nx + xg1;
+            float acc[NT][4];
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+            for (int k = 0; k < 9; ++k)
+            {
+                const int dt = kOffT[k], dx = kOffX[k];
+                // ldmatrix row of this lane: window site (r + 1 + dt, xs + 1 + dx + (lane & 15)),
+                // channels 4 (lane / 16) .. +3 of each 8-channel k-step
+                const uint32_t* wrow = tile + ((r + 1 + dt) * TW + xs + 1 + dx + (lane & 15)) * SW + (lane >> 4) * 4;
+                float P[NT][4];
+#pragma unroll
+                for (int n = 0; n < NT; ++n)
+                    P[n][0] = P[n][1] = P[n][2] = P[n][3] = 0.f;
+                for (int ks = 0; ks < ks_per; ++ks)
+                {
+                    uint32_t A[4];
+                    ldmatrix_x4(A, wrow + ks * 8);
+                    const uint2* bp = Bs + ((k * ks_per + ks) * NT) * 32 + lane;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n)
+                    {
+                        const uint2 b = bp[n * 32];
+                        mma_bf16(P[n], A[0], A[1], A[2], A[3], b.x, b.y);
+                    }
+                }
+                const float2 T0 = ok0 ? Tc[long(h0) * 9 + k] : make_float2(0.f, 0.f);
+                const float2 T1 = ok1 ? Tc[long(h1) * 9 + k] : make_float2(0.f, 0.f);
+#pragma unroll
+                for (int n = 0; n < NT; ++n)
+                {
+                    acc[n][0] += T0.x * P[n][0] - T0.y * P[n][1];
+                    acc[n][1] += T0.x * P[n][1] + T0.y * P[n][0];
+                    acc[n][2] += T1.x * P[n][2] - T1.y * P[n][3];
+                    acc[n][3] += T1.x * P[n][3] + T1.y * P[n][2];
+                }
+            }
 #pragma unroll
             for (int n = 0; n < NT; ++n)
             {
-                const uint2 b = bp[n * 32];
-                mma_bf16(acc[n], A0, A1, A2, A3, b.x, b.y);
+                const int o = 4 * n + q;
+                if (o < a.cout)
+                {
+                    const long off = chan_off(a.lo, o);
+                    if (ok0)
+                        outr[long(h0) * a.lo.hs + off] = make_float2(acc[n][0], acc[n][1]);
+                    if (ok1)
+                        outr[long(h1) * a.lo.hs + off] = make_float2(acc[n][2], acc[n][3]);
+                }
             }
         }
-        float2* outr = a.out + long(rhs) * a.lo.rs;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PTC layer on the 5th-generation tensor cores (tcgen05, accumulators in TMEM)
+// ---------------------------------------------------------------------------
+// A CTA of 4 warps owns a tile of 128 consecutive lattice sites (lexicographic
+// h = t Nx + x) of one right-hand side. The input around the tile (sites
+// h0 - Nx .. h0 + 127 + Nx) is staged in shared memory as BF16 in three
+// copies, copy dx holding in(t, x + dx) at the position of (t, x), so that
+// the operand of every offset (dt, dx) is a contiguous 128-row window of one
+// copy, (1 + dt) Nx rows from its start. Layout of a copy: planes of 4
+// complex channels (16 B per site), the canonical no-swizzle K-major layout
+// of tcgen05.mma (rows 16 B apart, 8-row groups 128 B apart, the two 16-B
+// K-chunks of a k-step one plane apart). The weights are the B operand
+// (N = 2 cout real columns, K-major). One elected thread issues, per offset,
+// cpad/8 MMAs of 128 x N x 16 into one of two TMEM accumulators and commits
+// them to an mbarrier; meanwhile the 4 warps read the other accumulator
+// (tcgen05.ld, one row per thread), multiply by that row's FP32 transporter
+// and add into FP32 registers.
+struct TcArgs
+{
+    const float2* in;
+    float2* out;
+    FieldLayout li, lo;
+    int cin, cout, cpad, ncol;   // ncol: real output columns (multiple of 16)
+    const uint4* B;              // [9 cpad/8][2][ncol] x 8 BF16
+    const float2* T;
+    const int* conf;
+    int conf0;
+    int Nt, Nx, V, nrhs;
+    int* err;
+    unsigned long long timeout_ns;
+    // BF16 planar fields ([rhs][plane][site] x 16 B, 4 channels per plane):
+    // when set, the input is read from in_bf (cp.async) instead of `in`, and
+    // the output written to out_bf instead of `out`
+    const uint4* in_bf;
+    uint4* out_bf;
+};
+
+constexpr int kTcM = 128;
+
+__host__ __device__ __forceinline__ size_t tc_smem_bytes(int cpad, int ncol, int Nx)
+{
+    const size_t J = size_t(kTcM) + 2 * size_t(Nx);
+    return size_t(9) * (cpad / 8) * 2 * ncol * 16 + size_t(3) * (cpad / 4) * J * 16;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, no swizzle (start, leading and stride byte
+// offsets in 16-B units; version 1).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u),
+          "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, unsigned long long limit_ns)
+{
+    const unsigned long long t0 = globaltimer_ns();
+    while (true)
+    {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done)
+            return true;
+        if (globaltimer_ns() - t0 > limit_ns)
+            return false;
+    }
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+#define DWFB_R8(i) "=r"(v[i]), "=r"(v[i + 1]), "=r"(v[i + 2]), "=r"(v[i + 3]), "=r"(v[i + 4]), \
+                   "=r"(v[i + 5]), "=r"(v[i + 6]), "=r"(v[i + 7])
+
+// 32 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+        "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : DWFB_R8(0), DWFB_R8(8), DWFB_R8(16), DWFB_R8(24)
+        : "r"(taddr));
+}
+#undef DWFB_R8
+
+#define DWFB_R8(i) "=r"(v[i]), "=r"(v[i + 1]), "=r"(v[i + 2]), "=r"(v[i + 3]), "=r"(v[i + 4]), \
+                   "=r"(v[i + 5]), "=r"(v[i + 6]), "=r"(v[i + 7])
+// 16 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+        "%15}, [%16];\n"
+        : DWFB_R8(0), DWFB_R8(8)
+        : "r"(taddr));
+}
+#undef DWFB_R8
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+constexpr int kTcThreads = 256;
+
+// Load 4 consecutive channels (one 16-B plane entry, BF16) of site h.
+__device__ __forceinline__ uint4 load_plane(const float2* __restrict__ inr, const FieldLayout& L, int cin,
+                                            long h, int c0)
+{
+    uint32_t w[4];
+    if (c0 + 3 < cin && L.cg % 4 == 0)
+    {
+        // 4 channels contiguous (network layout)
+        const float4* p = reinterpret_cast<const float4*>(inr + h * L.hs + chan_off(L, c0));
+        const float4 u = p[0], v = p[1];
+        w[0] = pack_bf2(u.x, u.y);
+        w[1] = pack_bf2(u.z, u.w);
+        w[2] = pack_bf2(v.x, v.y);
+        w[3] = pack_bf2(v.z, v.w);
+    }
+    else
+    {
 #pragma unroll
-        for (int n = 0; n < NT; ++n)
+        for (int q = 0; q < 4; q += 2)
         {
-            const int o = 4 * n + q;
-            if (o < a.cout)
+            const int c = c0 + q;
+            w[q] = w[q + 1] = 0u;
+            if (c + 1 < cin && L.cg % 2 == 0)
             {
-                const long off = chan_off(a.lo, o);
-                if (h0 + g < a.V)
-                    outr[long(h0 + g) * a.lo.hs + off] = make_float2(acc[n][0], acc[n][1]);
-                if (h0 + g + 8 < a.V)
-                    outr[long(h0 + g + 8) * a.lo.hs + off] = make_float2(acc[n][2], acc[n][3]);
+                // channel pair contiguous (operator layout: the two spins of one slice)
+                const float4 u = *reinterpret_cast<const float4*>(inr + h * L.hs + chan_off(L, c));
+                w[q] = pack_bf2(u.x, u.y);
+                w[q + 1] = pack_bf2(u.z, u.w);
+            }
+            else if (c < cin)
+            {
+                const float2 u = inr[h * L.hs + chan_off(L, c)];
+                w[q] = pack_bf2(u.x, u.y);
+                if (c + 1 < cin)
+                {
+                    const float2 u1 = inr[h * L.hs + chan_off(L, c + 1)];
+                    w[q + 1] = pack_bf2(u1.x, u1.y);
+                }
             }
         }
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+// Wait for the phase of `parity` of an mbarrier: poll (try_wait suspends
+// between polls), reading the timer only every 64 polls; false on timeout.
+__device__ __forceinline__ bool mbar_wait_lean(uint32_t mbar, uint32_t parity, unsigned long long limit_ns)
+{
+    unsigned long long t0 = 0;
+    for (int it = 0;; ++it)
+    {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done)
+            return true;
+        if ((it & 63) == 0)
+        {
+            const unsigned long long t = globaltimer_ns();
+            if (it == 0)
+                t0 = t;
+            else if (t - t0 > limit_ns)
+                return false;
+        }
+    }
+}
+
+// Stage the three x-shifted BF16 copies of the tile's input window.
+template <bool kPlanar>
+__device__ __forceinline__ void tc_stage(const TcArgs& a, uint4* As, int J, int planes, int h0, int rhs)
+{
+    const int nthr = blockDim.x;
+    for (int j = threadIdx.x; j < J; j += nthr)
+    {
+        int hs = h0 - a.Nx + j;
+        hs = hs < 0 ? hs + a.V : (hs >= a.V ? hs - a.V : hs);
+        hs = hs >= a.V ? hs % a.V : hs;  // tiles shorter than a row pair on tiny lattices
+        const int t = hs / a.Nx, x = hs - t * a.Nx;
+        const int row = t * a.Nx;
+        const int xm = (x == 0) ? a.Nx - 1 : x - 1;
+        const int xp = (x == a.Nx - 1) ? 0 : x + 1;
+        const int src[3] = {row + xm, row + x, row + xp};
+#pragma unroll
+        for (int dxi = 0; dxi < 3; ++dxi)
+        {
+            if (kPlanar)
+            {
+                const uint4* base = a.in_bf + long(rhs) * planes * a.V + src[dxi];
+                for (int pl = 0; pl < planes; ++pl)
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                     smem_u32(As + (dxi * planes + pl) * J + j)),
+                                 "l"(base + long(pl) * a.V)
+                                 : "memory");
+            }
+            else
+            {
+                const float2* inr = a.in + long(rhs) * a.li.rs;
+                for (int pl = 0; pl < planes; ++pl)
+                    As[(dxi * planes + pl) * J + j] = load_plane(inr, a.li, a.cin, src[dxi], 4 * pl);
+            }
+        }
+    }
+}
+
+// Offsets in the order the MMAs consume them: dx = -1 (copy 0), dx = 0
+// (copy 1), dx = +1 (copy 2), so that each copy is released for the next tile
+// after its third offset.
+__constant__ int kTcOrder[9] = {4, 6, 8, 0, 1, 2, 3, 5, 7};
+
+// Warp roles of the tcgen05 layer kernel (kTcThreads = 256):
+//   warps 0-3  epilogue: one TMEM lane (output site) per thread, all columns
+//   warp 4     MMA issue (one elected thread)
+//   warps 5-7  producers: stage copy c of the next tile into shared memory as
+//              soon as the MMAs of the current tile are done with it
+// mbarriers: tfull[s] / tempty[s] per TMEM slot, cfull[c] / cfree[c] per copy.
+constexpr int kEpiWarps = 4;
+constexpr int kProdWarps = 3;
+
+template <int NCOL>
+__global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int kSlots = 4;
+    __shared__ __align__(8) uint64_t mbar[2 * kSlots + 6];
+    __shared__ uint32_t tmem_holder;
+    constexpr int NC = NCOL / 2;
+    constexpr uint32_t kCols = (kSlots * NCOL <= 64) ? 64u
+                               : (kSlots * NCOL <= 128) ? 128u
+                               : (kSlots * NCOL <= 256) ? 256u : 512u;
+    static_assert(NC >= 1 && kSlots * NCOL <= 512, "TMEM columns");
+    const int ksp = a.cpad / 8;
+    const int nks = 9 * ksp;
+    const int planes = a.cpad / 4;
+    const int J = kTcM + 2 * a.Nx;
+    uint4* Bs = reinterpret_cast<uint4*>(smem);
+    uint4* As = Bs + nks * 2 * NCOL;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t mb = smem_u32(&mbar[0]);
+    auto TFULL = [&](int sl) { return mb + 8u * uint32_t(sl); };
+    auto TEMPTY = [&](int sl) { return mb + 8u * uint32_t(kSlots + sl); };
+    auto CFULL = [&](int c) { return mb + 8u * uint32_t(2 * kSlots + c); };
+    auto CFREE = [&](int c) { return mb + 8u * uint32_t(2 * kSlots + 3 + c); };
+    for (int i = tid; i < nks * 2 * NCOL; i += blockDim.x)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(Bs + i)), "l"(a.B + i) : "memory");
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (tid == 0)
+    {
+        for (int i = 0; i < kSlots; ++i)
+        {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(TFULL(i)), "r"(1u));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(TEMPTY(i)), "r"(uint32_t(kEpiWarps)));
+        }
+        for (int c = 0; c < 3; ++c)
+        {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(CFULL(c)), "r"(uint32_t(kProdWarps * 32)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(CFREE(c)), "r"(1u));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_holder)),
+                     "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_holder;
+    const long tiles_per_rhs = (a.V + kTcM - 1) / kTcM;
+    const long ntiles = tiles_per_rhs * a.nrhs;
+    bool ok = true;
+
+    if (warp >= kEpiWarps + 1)
+    {
+        // ---- producers ----
+        const int pt = tid - (kEpiWarps + 1) * 32;  // 0 .. 95
+        const int nprod = kProdWarps * 32;
+        uint32_t free_ph = 0u;  // bit c: next cfree phase
+        long it = 0;
+        for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++it)
+        {
+            const int rhs = int(tl / tiles_per_rhs);
+            const int h0 = int(tl - long(rhs) * tiles_per_rhs) * kTcM;
+            for (int c = 0; c < 3; ++c)
+            {
+                if (it > 0)
+                {
+                    // the MMAs of the previous tile are done with copy c
+                    if (!mbar_wait_lean(CFREE(c), (free_ph >> c) & 1u, a.timeout_ns))
+                        ok = false;
+                    free_ph ^= 1u << c;
+                }
+                const int dx = c - 1;
+                for (int j = pt; j < J; j += nprod)
+                {
+                    int hs = h0 - a.Nx + j;
+                    hs = hs < 0 ? hs + a.V : (hs >= a.V ? hs - a.V : hs);
+                    hs = hs >= a.V ? hs % a.V : hs;
+                    const int t = hs / a.Nx, x = hs - t * a.Nx;
+                    int x2 = x + dx;
+                    x2 = x2 < 0 ? x2 + a.Nx : (x2 >= a.Nx ? x2 - a.Nx : x2);
+                    const int src = t * a.Nx + x2;
+                    if (a.in_bf)
+                    {
+                        const uint4* base = a.in_bf + long(rhs) * planes * a.V + src;
+                        for (int pl = 0; pl < planes; ++pl)
+                            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                             smem_u32(As + (c * planes + pl) * J + j)),
+                                         "l"(base + long(pl) * a.V)
+                                         : "memory");
+                    }
+                    else
+                    {
+                        const float2* inr = a.in + long(rhs) * a.li.rs;
+                        for (int pl = 0; pl < planes; ++pl)
+                            As[(c * planes + pl) * J + j] = load_plane(inr, a.li, a.cin, src, 4 * pl);
+                    }
+                }
+                if (a.in_bf)
+                {
+                    // arrives once this thread's copies have landed
+                    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(CFULL(c)) : "memory");
+                }
+                else
+                {
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive(CFULL(c));
+                }
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    }
+    else if (warp == kEpiWarps)
+    {
+        // ---- MMA issue ----
+        if (lane == 0)
+        {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(NCOL >> 3) << 17) |
+                                   (uint32_t(kTcM >> 4) << 24);
+            const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
+            const uint32_t a_lbo = uint32_t(J) * 16u;
+            const uint32_t b_lbo = uint32_t(NCOL) * 16u;
+            uint32_t full_ph = 0u;   // bit c: next cfull phase
+            uint32_t empty_ph = 0u;  // bit s: next tempty phase
+            uint32_t used = 0u;
+            uint32_t g = 0;          // offsets issued so far
+            for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x)
+            {
+                for (int q = 0; q < 9; ++q, ++g)
+                {
+                    const int c = q / 3;
+                    if (q % 3 == 0)
+                    {
+                        if (!mbar_wait_lean(CFULL(c), (full_ph >> c) & 1u, a.timeout_ns))
+                            ok = false;
+                        full_ph ^= 1u << c;
+                        // the producers' copies become visible to the tensor cores
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    }
+                    const int sl = int(g % kSlots);
+                    if (used & (1u << sl))
+                    {
+                        if (!mbar_wait_lean(TEMPTY(sl), (empty_ph >> sl) & 1u, a.timeout_ns))
+                            ok = false;
+                        empty_ph ^= 1u << sl;
+                    }
+                    used |= 1u << sl;
+                    tc_fence_after();
+                    const int k = kTcOrder[q];
+                    const int dt = kOffT[k];
+                    const uint32_t d_tmem = tmem + uint32_t(sl) * uint32_t(NCOL);
+                    for (int ks = 0; ks < ksp; ++ks)
+                    {
+                        const uint32_t aaddr = a_base + uint32_t((c * planes + 2 * ks) * J + (1 + dt) * a.Nx) * 16u;
+                        const uint32_t baddr = b_base + uint32_t((k * ksp + ks) * 2 * NCOL) * 16u;
+                        tc_mma(d_tmem, umma_desc(aaddr, a_lbo, 128u), umma_desc(baddr, b_lbo, 128u), idesc,
+                               ks > 0 ? 1u : 0u);
+                    }
+                    tc_commit(TFULL(sl));
+                    if (q % 3 == 2)
+                        tc_commit(CFREE(c));
+                }
+            }
+            // the copy-release arrivals of the last tile land before the CTA exits
+            const long mine = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
+            if (mine > 0)
+                for (int c = 0; c < 3; ++c)
+                    if (!mbar_wait_lean(CFREE(c), uint32_t((mine - 1) & 1), a.timeout_ns))
+                        ok = false;
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---- epilogue ----
+        const int erow = 32 * warp + lane;
+        uint32_t full_ph = 0u;  // bit s: next tfull phase
+        uint32_t g = 0;
+        for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x)
+        {
+            const int rhs = int(tl / tiles_per_rhs);
+            const int h0 = int(tl - long(rhs) * tiles_per_rhs) * kTcM;
+            const int cf = a.conf ? a.conf[rhs] : a.conf0;
+            const int hrow = h0 + erow;
+            const bool row_ok = hrow < a.V;
+            float2 Tk[9];
+            {
+                const float2* Tc = a.T + (long(cf) * a.V + (row_ok ? hrow : 0)) * 9;
+#pragma unroll
+                for (int q = 0; q < 9; ++q)
+                    Tk[q] = row_ok ? Tc[q] : make_float2(0.f, 0.f);
+            }
+            float acc[NC][2];
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc)
+                acc[cc][0] = acc[cc][1] = 0.f;
+#pragma unroll 1
+            for (int q = 0; q < 9; ++q, ++g)
+            {
+                const int sl = int(g % kSlots);
+                if (!mbar_wait_lean(TFULL(sl), (full_ph >> sl) & 1u, a.timeout_ns))
+                    ok = false;
+                full_ph ^= 1u << sl;
+                tc_fence_after();
+                const int k = kTcOrder[q];
+                float2 T = Tk[0];
+#pragma unroll
+                for (int u = 1; u < 9; ++u)
+                    T = (k == u) ? Tk[u] : T;
+                const uint32_t tbase = tmem + (uint32_t(32 * warp) << 16) + uint32_t(sl * NCOL);
+#pragma unroll
+                for (int c0 = 0; c0 < NCOL; c0 += 32)
+                {
+                    uint32_t v[32];
+                    if (c0 + 32 <= NCOL)
+                        tmem_ld32(tbase + uint32_t(c0), v);
+                    else
+                    {
+                        uint32_t w[16];
+                        tmem_ld16(tbase + uint32_t(c0), w);
+#pragma unroll
+                        for (int u = 0; u < 16; ++u)
+                            v[u] = w[u];
+                    }
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                    {
+                        if (c0 / 2 + u < NC)
+                        {
+                            const float pr = __uint_as_float(v[2 * u]), pi = __uint_as_float(v[2 * u + 1]);
+                            acc[c0 / 2 + u][0] += T.x * pr - T.y * pi;
+                            acc[c0 / 2 + u][1] += T.x * pi + T.y * pr;
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0)
+                    mbar_arrive(TEMPTY(sl));
+            }
+            if (row_ok)
+            {
+                if (a.out_bf)
+                {
+                    const int planes_out = (a.cout + 7) / 8 * 2;
+                    uint4* ob = a.out_bf + long(rhs) * planes_out * a.V + hrow;
+#pragma unroll
+                    for (int cc = 0; cc < NC; cc += 4)
+                    {
+                        uint32_t w[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            w[u] = (cc + u < a.cout && cc + u < NC) ? pack_bf2(acc[cc + u][0], acc[cc + u][1]) : 0u;
+                        if (cc / 4 < planes_out)
+                            ob[long(cc / 4) * a.V] = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                }
+                else
+                {
+                    float2* outr = a.out + long(rhs) * a.lo.rs + long(hrow) * a.lo.hs;
+#pragma unroll
+                    for (int cc = 0; cc < NC; ++cc)
+                        if (cc < a.cout)
+                            outr[chan_off(a.lo, cc)] = make_float2(acc[cc][0], acc[cc][1]);
+                }
+            }
+        }
+    }
+    if (!ok && a.err)
+        atomicExch(a.err, DWF_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+
+// FP32 field (any layout) -> BF16 planar [rhs][plane][site].
+__global__ void lp_to_planar_kernel(const float2* __restrict__ in, FieldLayout L, int cin, int planes, int V,
+                                    int nrhs, uint4* __restrict__ out)
+{
+    const long n = long(nrhs) * planes * V;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const int h = int(i % V);
+        const long r = i / V;
+        const int pl = int(r % planes), rhs = int(r / planes);
+        out[i] = load_plane(in + long(rhs) * L.rs, L, cin, h, 4 * pl);
+    }
+}
+
+// Weights in the tcgen05 B layout: element (k-step ks, K-chunk ch, column n,
+// e) is BF16 number 8 ch + e of the k-step's reduction index (activation
+// j = 8 ks + (8 ch + e) / 2, real part for even e) against real column n.
+__global__ void lp_pack_tc_kernel(const float2* __restrict__ W, int cin, int cout, int adjoint, int cpad,
+                                  int ncol, __nv_bfloat16* __restrict__ B)
+{
+    const int ci = adjoint ? cout : cin;
+    const int co = adjoint ? cin : cout;
+    const int nks = 9 * cpad / 8;
+    const long total = long(nks) * 2 * ncol * 8;
+    for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < total; idx += long(gridDim.x) * blockDim.x)
+    {
+        const int e = int(idx & 7);
+        const long r = idx >> 3;
+        const int n = int(r % ncol);
+        const int ch = int((r / ncol) & 1);
+        const int ks = int(r / (2L * ncol));
+        const int kk = 8 * ch + e;
+        const int j = 8 * ks + (kk >> 1);
+        const int k = j / cpad, i = j - k * cpad;
+        const int o = n >> 1;
+        float2 w = make_float2(0.f, 0.f);
+        if (o < co && i < ci)
+        {
+            if (!adjoint)
+                w = W[(long(k) * cout + o) * cin + i];
+            else
+            {
+                const int kr = (k == 0) ? 0 : ((k <= 4) ? ((k & 1) ? k + 1 : k - 1) : 13 - k);
+                const float2 u = W[(long(kr) * cout + i) * cin + o];
+                w = make_float2(u.x, -u.y);
+            }
+        }
+        float val;
+        if ((n & 1) == 0)
+            val = (kk & 1) ? -w.y : w.x;
+        else
+            val = (kk & 1) ? w.x : w.y;
+        B[idx] = __float2bfloat16_rn(val);
     }
 }
 
@@ -394,9 +1028,9 @@ __global__ void __launch_bounds__(kGradThreads) lp_wgrad_kernel(GradArgs a)
                     xx = xx < 0 ? xx + a.Nx : (xx >= a.Nx ? xx - a.Nx : xx);
                     const float2 T = Tc[long(h) * 9 + k];
                     const float2 u = inr[long(tt * a.Nx + xx) * a.li.hs + chan_off(a.li, i)];
-                    const uint32_t b = transported(T, u);
-                    const __nv_bfloat162 bb = *reinterpret_cast<const __nv_bfloat162*>(&b);
-                    v = __bfloat1622float2(bb);
+                    const uint32_t b = pack_bf2(u.x, u.y);
+                    const float2 ub = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&b));
+                    v = make_float2(T.x * ub.x - T.y * ub.y, T.x * ub.y + T.y * ub.x);
                 }
                 as[e] = v;
             }
@@ -857,7 +1491,7 @@ __global__ void lp_diff_kernel(const double2* __restrict__ a, const double2* __r
 struct LpNet
 {
     int C0 = 0, H = 0;
-    int cin[kLpLayers], cout[kLpLayers], ksteps[kLpLayers], ntf[kLpLayers], nta[kLpLayers];
+    int cin[kLpLayers], cout[kLpLayers], ntf[kLpLayers], nta[kLpLayers];
     long woff[kLpLayers + 1];          // complex offsets of each layer's weights
     long bf_off[kLpLayers + 1];        // uint2 offsets of forward fragments
     long ba_off[kLpLayers + 1];        // and of adjoint fragments
@@ -868,6 +1502,13 @@ struct LpNet
     long adam_t = 0;
     uint2* Bf = nullptr;
     uint2* Ba = nullptr;
+    // tcgen05 B operands (forward and adjoint) and their real column counts
+    uint4* Btf = nullptr;
+    uint4* Bta = nullptr;
+    long tf_off[kLpLayers + 1], ta_off[kLpLayers + 1];
+    int ncf[kLpLayers], nca[kLpLayers];
+    int variant = -1;                  // -1 auto, 0 mma.sync kernel, 1 tcgen05 kernel
+    int* err_d = nullptr;              // bounded-wait error flag of the tcgen05 kernel
     float2* T = nullptr;               // transports [nconf][V][9]
     int T_cap = 0;
     uint64_t T_version = ~0ull;
@@ -875,6 +1516,7 @@ struct LpNet
     int act_rhs = 0;
     float2* act[kLpLayers] = {nullptr, nullptr, nullptr, nullptr};
     float2* hid[2] = {nullptr, nullptr};
+    uint4* hb[2] = {nullptr, nullptr};  // BF16 planar hidden fields (tcgen05 chain)
     float2* gbuf[2] = {nullptr, nullptr};   // gradients flowing back (operator and hidden layout)
     float2* gpart = nullptr;
     size_t gpart_cap = 0;
@@ -922,19 +1564,27 @@ int lp_grow(dwf_ctx* c, T*& p, size_t n)
 
 int nt_of(int cout) { return (2 * cout + 7) / 8; }
 
+int ncol_of(int cout) { return (2 * cout + 15) / 16 * 16; }
+
 int grid_for(long n, int nsm) { return int(std::max<long>(1, std::min<long>((n + 255) / 256, 8L * nsm))); }
 
-int set_ptc_smem(dwf_ctx* c)
+int cpad_of(int c) { return (c + 7) / 8 * 8; }
+
+int set_conv_smem(dwf_ctx* c)
 {
     static int done_dev = -1;
     if (done_dev == c->device)
         return DWF_OK;
-    const int mx = 200 * 1024;
-    CK(cudaFuncSetAttribute(lp_ptc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(lp_ptc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(lp_ptc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(lp_ptc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(lp_ptc_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    const int mx = 220 * 1024;
+    CK(cudaFuncSetAttribute(lp_conv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_conv_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_conv_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_conv_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_conv_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_tc_kernel<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     done_dev = c->device;
     return DWF_OK;
 }
@@ -948,12 +1598,21 @@ int lp_pack(dwf_ctx* c)
         const long nf = n->bf_off[l + 1] - n->bf_off[l];
         const long na = n->ba_off[l + 1] - n->ba_off[l];
         lp_pack_kernel<<<grid_for(nf, c->nsm), 256, 0, c->stream>>>(
-            n->W + n->woff[l], n->cin[l], n->cout[l], 0, n->ksteps[l], n->ntf[l], n->Bf + n->bf_off[l]);
+            n->W + n->woff[l], n->cin[l], n->cout[l], 0, cpad_of(n->cin[l]), n->ntf[l],
+            n->Bf + n->bf_off[l]);
         // adjoint layer: cin' = cout, cout' = cin
         lp_pack_kernel<<<grid_for(na, c->nsm), 256, 0, c->stream>>>(
-            n->W + n->woff[l], n->cin[l], n->cout[l], 1, (9 * n->cout[l] + 7) / 8, n->nta[l],
+            n->W + n->woff[l], n->cin[l], n->cout[l], 1, cpad_of(n->cout[l]), n->nta[l],
             n->Ba + n->ba_off[l]);
-        c->launches += 2;
+        const long tf = (n->tf_off[l + 1] - n->tf_off[l]) * 8;
+        const long ta = (n->ta_off[l + 1] - n->ta_off[l]) * 8;
+        lp_pack_tc_kernel<<<grid_for(tf, c->nsm), 256, 0, c->stream>>>(
+            n->W + n->woff[l], n->cin[l], n->cout[l], 0, cpad_of(n->cin[l]), n->ncf[l],
+            reinterpret_cast<__nv_bfloat16*>(n->Btf + n->tf_off[l]));
+        lp_pack_tc_kernel<<<grid_for(ta, c->nsm), 256, 0, c->stream>>>(
+            n->W + n->woff[l], n->cin[l], n->cout[l], 1, cpad_of(n->cout[l]), n->nca[l],
+            reinterpret_cast<__nv_bfloat16*>(n->Bta + n->ta_off[l]));
+        c->launches += 4;
     }
     CK(cudaGetLastError());
     return DWF_OK;
@@ -1004,19 +1663,77 @@ FieldLayout op_layout(const dwf_ctx* c)
 
 FieldLayout net_layout(const dwf_ctx* c, int C) { return FieldLayout{long(c->L.V) * C, C, C, 0}; }
 
-// One layer (forward or adjoint) on device fields.
+// Whether the tcgen05 kernel takes layer l (its shared-memory tile fits).
+bool tc_fits(const dwf_ctx* c, int l, bool adjoint)
+{
+    const LpNet* n = c->lp;
+    const int ci = adjoint ? n->cout[l] : n->cin[l];
+    const int co = adjoint ? n->cin[l] : n->cout[l];
+    const int ncol = ncol_of(co);
+    return ncol <= 96 && tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx) <= size_t(220 * 1024);
+}
+
+// One layer (forward or adjoint) on device fields. in_bf / out_bf (tcgen05
+// kernel only): BF16 planar input / output in place of in / out.
 int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const float2* in,
-             FieldLayout li, float2* out, FieldLayout lo)
+             FieldLayout li, float2* out, FieldLayout lo, const uint4* in_bf = nullptr,
+             uint4* out_bf = nullptr)
 {
     LpNet* n = c->lp;
-    PtcArgs a;
+    const int ci = adjoint ? n->cout[l] : n->cin[l];
+    const int co = adjoint ? n->cin[l] : n->cout[l];
+    const int ncol = ncol_of(co);
+    const size_t tsm = tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx);
+    const bool tc_ok = tc_fits(c, l, adjoint);
+    if (n->variant != 0 && tc_ok)
+    {
+        TcArgs t;
+        t.in = in;
+        t.out = out;
+        t.li = li;
+        t.lo = lo;
+        t.cin = ci;
+        t.cout = co;
+        t.cpad = cpad_of(ci);
+        t.ncol = ncol;
+        t.B = adjoint ? n->Bta + n->ta_off[l] : n->Btf + n->tf_off[l];
+        t.T = n->T;
+        t.conf = conf_d;
+        t.conf0 = 0;
+        t.Nt = c->L.Nt;
+        t.Nx = c->L.Nx;
+        t.V = c->L.V;
+        t.nrhs = nrhs;
+        t.err = n->err_d;
+        t.timeout_ns = c->timeout_ns;
+        t.in_bf = in_bf;
+        t.out_bf = out_bf;
+        const long ntiles = long((c->L.V + kTcM - 1) / kTcM) * nrhs;
+        const int grid = int(std::max<long>(1, std::min<long>(ntiles, long(c->nsm))));
+        ST(set_conv_smem(c));
+        switch (ncol)
+        {
+        case 16: lp_tc_kernel<16><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
+        case 32: lp_tc_kernel<32><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
+        case 64: lp_tc_kernel<64><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
+        case 96: lp_tc_kernel<96><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
+        default: return ctx_fail(c, DWF_BAD_ARG, "learned: unsupported channel count");
+        }
+        c->launches += 1;
+        CK(cudaGetLastError());
+        return DWF_OK;
+    }
+    if (n->variant == 1 || in_bf || out_bf)
+        return ctx_fail(c, DWF_BAD_ARG, "learned: the tcgen05 layer does not fit this lattice / width");
+    ConvArgs a;
     a.in = in;
     a.out = out;
     a.li = li;
     a.lo = lo;
     a.cin = adjoint ? n->cout[l] : n->cin[l];
     a.cout = adjoint ? n->cin[l] : n->cout[l];
-    a.ksteps = (9 * a.cin + 7) / 8;
+    a.cpad = cpad_of(a.cin);
+    a.tx = std::min(64, (c->L.Nx + 15) / 16 * 16);
     a.B = adjoint ? n->Ba + n->ba_off[l] : n->Bf + n->bf_off[l];
     a.T = n->T;
     a.conf = conf_d;
@@ -1026,17 +1743,17 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
     a.V = c->L.V;
     a.nrhs = nrhs;
     const int nt = nt_of(a.cout);
-    const size_t smem = ptc_smem_bytes(a.ksteps, nt);
-    const long ntiles = long((a.V + 15) / 16) * nrhs;
-    const int grid = int(std::max<long>(1, std::min<long>((ntiles + kPtcWarps - 1) / kPtcWarps, 3L * c->nsm)));
-    ST(set_ptc_smem(c));
+    const size_t smem = conv_smem_bytes(a.cpad, nt, a.tx);
+    const long ntiles = long((a.Nt + kTileRows - 1) / kTileRows) * ((a.Nx + a.tx - 1) / a.tx) * nrhs;
+    const int grid = int(std::max<long>(1, std::min<long>(ntiles, 2L * c->nsm)));
+    ST(set_conv_smem(c));
     switch (nt)
     {
-    case 1: lp_ptc_kernel<1><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
-    case 2: lp_ptc_kernel<2><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
-    case 4: lp_ptc_kernel<4><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
-    case 8: lp_ptc_kernel<8><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
-    case 12: lp_ptc_kernel<12><<<grid, kPtcWarps * 32, smem, c->stream>>>(a); break;
+    case 1: lp_conv_kernel<1><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
+    case 2: lp_conv_kernel<2><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
+    case 4: lp_conv_kernel<4><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
+    case 8: lp_conv_kernel<8><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
+    case 12: lp_conv_kernel<12><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
     default: return ctx_fail(c, DWF_BAD_ARG, "learned: unsupported channel count");
     }
     c->launches += 1;
@@ -1057,6 +1774,9 @@ int lp_ensure_act(dwf_ctx* c, int nrhs)
     ST(lp_grow(c, n->hid[1], std::max(hid, op)));
     ST(lp_grow(c, n->gbuf[0], std::max(hid, op)));
     ST(lp_grow(c, n->gbuf[1], std::max(hid, op)));
+    const size_t pl = size_t(std::max(cpad_of(n->C0), cpad_of(n->H)) / 4);
+    ST(lp_grow(c, n->hb[0], size_t(nrhs) * pl * c->L.V));
+    ST(lp_grow(c, n->hb[1], size_t(nrhs) * pl * c->L.V));
     n->act_rhs = nrhs;
     return DWF_OK;
 }
@@ -1070,6 +1790,28 @@ int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* 
     LpNet* n = c->lp;
     ST(lp_ensure_act(c, nrhs));
     const FieldLayout lop = op_layout(c), lh = net_layout(c, n->H);
+    bool chain = !keep && n->variant != 0;
+    for (int l = 0; l < kLpLayers; ++l)
+        chain = chain && tc_fits(c, l, adjoint);
+    if (chain)
+    {
+        // tcgen05 chain: BF16 planar activations between the layers
+        const int l0 = adjoint ? kLpLayers - 1 : 0;
+        const int cin0 = adjoint ? n->cout[l0] : n->cin[l0];
+        const int planes0 = cpad_of(cin0) / 4;
+        const long np = long(nrhs) * planes0 * c->L.V;
+        lp_to_planar_kernel<<<grid_for(np, c->nsm), 256, 0, c->stream>>>(in, lop, cin0, planes0, c->L.V,
+                                                                          nrhs, n->hb[0]);
+        c->launches += 1;
+        for (int s = 0; s < kLpLayers; ++s)
+        {
+            const int l = adjoint ? kLpLayers - 1 - s : s;
+            const bool last = (s == kLpLayers - 1);
+            ST(lp_layer(c, l, adjoint, nrhs, conf_d, nullptr, lop, last ? out : nullptr, lop, n->hb[s & 1],
+                        last ? nullptr : n->hb[(s + 1) & 1]));
+        }
+        return DWF_OK;
+    }
     const float2* cur = in;
     FieldLayout lcur = lop;
     for (int s = 0; s < kLpLayers; ++s)
@@ -1207,6 +1949,20 @@ int lp_ensure_solver(dwf_ctx* c, int nrhs)
     return DWF_OK;
 }
 
+// DWF_TIMEOUT (and the flag cleared) if a tcgen05 layer gave up a bounded wait.
+int lp_check_err(dwf_ctx* c)
+{
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, c->lp->err_d, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (e)
+    {
+        CK(cudaMemsetAsync(c->lp->err_d, 0, sizeof(int), c->stream));
+        return ctx_fail(c, DWF_TIMEOUT, "learned: a tensor-core layer timed out waiting for its MMAs");
+    }
+    return DWF_OK;
+}
+
 // Gaussian FP64 fields (n complex numbers) on the device.
 int lp_gauss(dwf_ctx* c, double2* out, long n, uint64_t seed)
 {
@@ -1223,7 +1979,7 @@ void lp_destroy(dwf_ctx* c)
     LpNet* n = c->lp;
     if (!n)
         return;
-    void* bufs[] = {n->W, n->G, n->m, n->v, n->Bf, n->Ba, n->T, n->act[1], n->act[2], n->act[3],
+    void* bufs[] = {n->W, n->G, n->m, n->v, n->Bf, n->Ba, n->Btf, n->Bta, n->err_d, n->hb[0], n->hb[1], n->T, n->act[1], n->act[2], n->act[3],
                     n->hid[0], n->hid[1], n->gbuf[0], n->gbuf[1], n->gpart, n->lpart, n->lscale,
                     n->dloss, n->dconf, n->pr_rho, n->pr_e, n->s_r64, n->s_t64, n->s_rhs64,
                     n->s_part2, n->s_part, n->s_val, n->s_state};
@@ -1374,6 +2130,7 @@ int lp_solve(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double
         c->launches += 1;
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(c->stream));
+        ST(lp_check_err(c));
         for (int k = 0; k < nrhs; ++k)
             if (scale[k] > 0.0)
             {
@@ -1452,12 +2209,17 @@ int dwf_lp_init(dwf_ctx* c, int hidden, uint64_t seed)
     {
         n->cin[l] = ch[l];
         n->cout[l] = ch[l + 1];
-        n->ksteps[l] = (9 * ch[l] + 7) / 8;
         n->ntf[l] = nt_of(ch[l + 1]);
         n->nta[l] = nt_of(ch[l]);
         n->woff[l + 1] = n->woff[l] + 9L * ch[l] * ch[l + 1];
-        n->bf_off[l + 1] = n->bf_off[l] + long(n->ksteps[l]) * n->ntf[l] * 32;
-        n->ba_off[l + 1] = n->ba_off[l] + long((9 * ch[l + 1] + 7) / 8) * n->nta[l] * 32;
+        n->bf_off[l + 1] = n->bf_off[l] + 9L * (cpad_of(ch[l]) / 8) * n->ntf[l] * 32;
+        n->ba_off[l + 1] = n->ba_off[l] + 9L * (cpad_of(ch[l + 1]) / 8) * n->nta[l] * 32;
+        n->ncf[l] = ncol_of(ch[l + 1]);
+        n->nca[l] = ncol_of(ch[l]);
+        if (l == 0)
+            n->tf_off[0] = n->ta_off[0] = 0;
+        n->tf_off[l + 1] = n->tf_off[l] + 9L * (cpad_of(ch[l]) / 8) * 2 * n->ncf[l];
+        n->ta_off[l + 1] = n->ta_off[l] + 9L * (cpad_of(ch[l + 1]) / 8) * 2 * n->nca[l];
     }
     const long nw = n->woff[kLpLayers];
     ST(lp_grow(c, n->W, nw));
@@ -1466,6 +2228,10 @@ int dwf_lp_init(dwf_ctx* c, int hidden, uint64_t seed)
     ST(lp_grow(c, n->v, 2 * nw));
     ST(lp_grow(c, n->Bf, n->bf_off[kLpLayers]));
     ST(lp_grow(c, n->Ba, n->ba_off[kLpLayers]));
+    ST(lp_grow(c, n->Btf, n->tf_off[kLpLayers]));
+    ST(lp_grow(c, n->Bta, n->ta_off[kLpLayers]));
+    ST(lp_grow(c, n->err_d, 1));
+    CK(cudaMemsetAsync(n->err_d, 0, sizeof(int), c->stream));
     CK(cudaMemsetAsync(n->m, 0, 2 * nw * sizeof(float), c->stream));
     CK(cudaMemsetAsync(n->v, 0, 2 * nw * sizeof(float), c->stream));
     // initial weights: small seeded Gaussian noise, plus the identity on the
@@ -1542,7 +2308,7 @@ int dwf_lp_apply_dev(dwf_ctx* c, int adjoint, int nrhs, const int* rhs_conf, con
     ST(lp_conf(c, nrhs, rhs_conf, &conf_d));
     ST(lp_transports(c));
     ST(lp_net(c, adjoint != 0, nrhs, conf_d, static_cast<const float2*>(in), static_cast<float2*>(out), false));
-    return DWF_OK;
+    return lp_check_err(c);
 }
 
 int dwf_lp_layer_dev(dwf_ctx* c, int layer, int adjoint, int nrhs, const int* rhs_conf, const void* in,
@@ -1559,7 +2325,7 @@ int dwf_lp_layer_dev(dwf_ctx* c, int layer, int adjoint, int nrhs, const int* rh
     const int co = adjoint ? n->cin[layer] : n->cout[layer];
     ST(lp_layer(c, layer, adjoint != 0, nrhs, conf_d, static_cast<const float2*>(in), net_layout(c, ci),
                 static_cast<float2*>(out), net_layout(c, co)));
-    return DWF_OK;
+    return lp_check_err(c);
 }
 
 int dwf_lp_loss_grad_dev(dwf_ctx* c, int npair, const int* pair_conf, const void* rho, const void* e,
@@ -1572,6 +2338,7 @@ int dwf_lp_loss_grad_dev(dwf_ctx* c, int npair, const int* pair_conf, const void
     ST(lp_conf(c, npair, pair_conf, &conf_d));
     ST(lp_transports(c));
     ST(lp_loss_grad(c, npair, conf_d, static_cast<const float2*>(rho), static_cast<const float2*>(e), loss));
+    ST(lp_check_err(c));
     if (grad)
     {
         CK(cudaMemcpyAsync(grad, c->lp->G, c->lp->woff[kLpLayers] * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
@@ -1698,6 +2465,7 @@ int dwf_lp_train(dwf_ctx* c, const dwf_lp_train_params* tp, dwf_lp_train_info* t
     cudaFree(be);
     if (st != DWF_OK)
         return st;
+    ST(lp_check_err(c));
     const auto t2 = std::chrono::steady_clock::now();
     if (ti)
     {
@@ -1709,6 +2477,14 @@ int dwf_lp_train(dwf_ctx* c, const dwf_lp_train_params* tp, dwf_lp_train_info* t
         ti->seconds_pairs = std::chrono::duration<double>(t1 - t0).count();
         ti->seconds_train = std::chrono::duration<double>(t2 - t1).count();
     }
+    return DWF_OK;
+}
+
+int dwf_lp_set_variant(dwf_ctx* c, int variant)
+{
+    if (!c || !c->lp || variant < -1 || variant > 1)
+        return c ? ctx_fail(c, DWF_BAD_ARG, "dwf_lp_set_variant: bad variant or no network") : DWF_BAD_ARG;
+    c->lp->variant = variant;
     return DWF_OK;
 }
 

@@ -117,6 +117,10 @@ class LearnedMixin:
                                          _ptr(h) if h is not None else None))
         return (info.as_dict(), h) if history else info.as_dict()
 
+    def lp_set_variant(self, variant):
+        """Layer kernel: -1 automatic, 0 mma.sync, 1 tcgen05."""
+        self._check(A.lib().dwf_lp_set_variant(self._h, int(variant)))
+
     def lp_set_solver(self, inner_tol=1e-4, inner_maxiter=400, outer_max=40):
         self._check(A.lib().dwf_lp_set_solver(self._h, float(inner_tol), int(inner_maxiter),
                                               int(outer_max)))

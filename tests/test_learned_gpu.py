@@ -179,12 +179,14 @@ def point_sources(Nt, Nx, Ls, n):
 
 
 def test_learned_solve_meets_rule_and_matches_fp64(T):
+    """More right-hand sides (10) than the training batch (8): the solver's
+    buffers are sized for its own batch."""
     d, th, untrained, tinfo = learned_setup(T, 16, 16, 8, 3.0, 16, 600)
-    src = point_sources(16, 16, 8, 4)
-    conf = np.array([0, 1, 2, 3], np.int32)
+    src = point_sources(16, 16, 8, 10)
+    conf = np.arange(10, dtype=np.int32) % 4
     x, info = d.propagators(src, rhs_conf=conf, rtol=1e-10, maxiter=20000, solver=T.SOLVER_LEARNED)
     x64, i64 = d.propagators(src, rhs_conf=conf, rtol=1e-12, maxiter=40000, solver=T.SOLVER_CG64)
-    for k in range(4):
+    for k in range(10):
         assert info[k]["converged"] and info[k]["true_relres"] <= 1e-10, info[k]
         assert info[k]["solver"] == T.SOLVER_LEARNED and info[k]["fallback"] == 0
         assert rel(x[k], x64[k]) < 1e-7

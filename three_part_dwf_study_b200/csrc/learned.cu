@@ -1207,7 +1207,7 @@ struct Dot
 };
 
 // part[((slot * nrhs + rhs) * nblk + blk)] = <a, b> over this block's chunk,
-// for up to three pairs.
+// for up to three pairs, in one pass over the data.
 __global__ void lp_dots_kernel(Dot d0, Dot d1, Dot d2, int ndot, long fsz, int nblk,
                                double2* __restrict__ part)
 {
@@ -1217,20 +1217,27 @@ __global__ void lp_dots_kernel(Dot d0, Dot d1, Dot d2, int ndot, long fsz, int n
     const long ch = (fsz + nblk - 1) / nblk;
     const long i0 = blockIdx.x * ch, i1 = (i0 + ch < fsz) ? i0 + ch : fsz;
     const long base = long(rhs) * fsz;
+    double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
+    for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+    {
+#pragma unroll
+        for (int s = 0; s < 3; ++s)
+        {
+            if (s < ndot)
+            {
+                const Dot d = s == 0 ? d0 : (s == 1 ? d1 : d2);
+                const float2 x = d.a[base + i], y = d.b[base + i];
+                re[s] += double(x.x) * y.x + double(x.y) * y.y;
+                im[s] += double(x.x) * y.y - double(x.y) * y.x;
+            }
+        }
+    }
     for (int s = 0; s < ndot; ++s)
     {
-        const Dot d = s == 0 ? d0 : (s == 1 ? d1 : d2);
-        double re = 0.0, im = 0.0;
-        for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x)
-        {
-            const float2 x = d.a[base + i], y = d.b[base + i];
-            re += double(x.x) * y.x + double(x.y) * y.y;
-            im += double(x.x) * y.y - double(x.y) * y.x;
-        }
-        re = block_sum(re, red);
-        im = block_sum(im, red);
+        const double r = block_sum(re[s], red);
+        const double m = block_sum(im[s], red);
         if (threadIdx.x == 0)
-            part[(long(s) * nrhs + rhs) * nblk + blockIdx.x] = make_double2(re, im);
+            part[(long(s) * nrhs + rhs) * nblk + blockIdx.x] = make_double2(r, m);
     }
 }
 
@@ -1394,6 +1401,99 @@ __global__ void lp_bs_vec_kernel(int op, long fsz, int nrhs, const BsState* __re
     }
 }
 
+// Fused BiCGStab updates with the network's BF16 planar input (4 channels of
+// one site per thread; channel c = 2 slice + spin of the operator layout).
+// op 0: p = r + beta (p - omega v), planar(p)
+// op 1: s = r - alpha v,            planar(s)
+__global__ void lp_bs_planar_kernel(int op, int Ls, int V, int planes, int nrhs, const BsState* __restrict__ S,
+                                    float2* __restrict__ p, const float2* __restrict__ r,
+                                    const float2* __restrict__ v, float2* __restrict__ s,
+                                    uint4* __restrict__ planar)
+{
+    const long fsz = 2L * Ls * V;
+    const long n = long(nrhs) * planes * V;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const int h = int(i % V);
+        const long q = i / V;
+        const int pl = int(q % planes), rhs = int(q / planes);
+        const BsState& st = S[rhs];
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            const int sl = 2 * pl + half;  // fifth-dimension slice: channels 2 sl, 2 sl + 1
+            if (sl >= Ls)
+                continue;
+            const long e = long(rhs) * fsz + (long(sl) * V + h) * 2;  // complex index of (slice, site, spin 0)
+            const float4 rv = *reinterpret_cast<const float4*>(r + e);
+            const float4 vv = *reinterpret_cast<const float4*>(v + e);
+            float4 o;
+            if (op == 0)
+            {
+                const float4 pv = *reinterpret_cast<const float4*>(p + e);
+                const float2 wo = fz(st.omega), b = fz(st.beta);
+                const float2 d0 = make_float2(pv.x - (wo.x * vv.x - wo.y * vv.y), pv.y - (wo.x * vv.y + wo.y * vv.x));
+                const float2 d1 = make_float2(pv.z - (wo.x * vv.z - wo.y * vv.w), pv.w - (wo.x * vv.w + wo.y * vv.z));
+                const float2 b0 = cmulf(b, d0), b1 = cmulf(b, d1);
+                o = make_float4(rv.x + b0.x, rv.y + b0.y, rv.z + b1.x, rv.w + b1.y);
+                *reinterpret_cast<float4*>(p + e) = o;
+            }
+            else
+            {
+                const float2 al = fz(st.alpha);
+                const float2 a0 = cmulf(al, make_float2(vv.x, vv.y)), a1 = cmulf(al, make_float2(vv.z, vv.w));
+                o = make_float4(rv.x - a0.x, rv.y - a0.y, rv.z - a1.x, rv.w - a1.y);
+                *reinterpret_cast<float4*>(s + e) = o;
+            }
+            w[2 * half] = pack_bf2(o.x, o.y);
+            w[2 * half + 1] = pack_bf2(o.z, o.w);
+        }
+        planar[(long(rhs) * planes + pl) * V + h] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// x += alpha ph + omega sh ; r = s - omega t ; partials of <rh, r>, <r, r>
+// (slots 0, 1) for the next coefficient step.
+__global__ void lp_bs_xr_kernel(long fsz, int nblk, const BsState* __restrict__ S, float2* __restrict__ x,
+                                const float2* __restrict__ ph, const float2* __restrict__ sh,
+                                const float2* __restrict__ s, const float2* __restrict__ t,
+                                float2* __restrict__ r, const float2* __restrict__ rh,
+                                double2* __restrict__ part)
+{
+    __shared__ double red[32];
+    const int rhs = blockIdx.y;
+    const int nrhs = gridDim.y;
+    const long ch = (fsz + nblk - 1) / nblk;
+    const long i0 = blockIdx.x * ch, i1 = (i0 + ch < fsz) ? i0 + ch : fsz;
+    const long base = long(rhs) * fsz;
+    const BsState st = S[rhs];
+    const float2 al = fz(st.alpha), wo = fz(st.omega);
+    double a_re = 0.0, a_im = 0.0, rr = 0.0;
+    for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+    {
+        const long k = base + i;
+        const float2 u1 = cmulf(al, ph[k]), u2 = cmulf(wo, sh[k]);
+        const float2 xv = x[k];
+        x[k] = make_float2(xv.x + u1.x + u2.x, xv.y + u1.y + u2.y);
+        const float2 sv = s[k], wt = cmulf(wo, t[k]);
+        const float2 rn = make_float2(sv.x - wt.x, sv.y - wt.y);
+        r[k] = rn;
+        const float2 hv = rh[k];
+        a_re += double(hv.x) * rn.x + double(hv.y) * rn.y;
+        a_im += double(hv.x) * rn.y - double(hv.y) * rn.x;
+        rr += double(rn.x) * rn.x + double(rn.y) * rn.y;
+    }
+    a_re = block_sum(a_re, red);
+    a_im = block_sum(a_im, red);
+    rr = block_sum(rr, red);
+    if (threadIdx.x == 0)
+    {
+        part[(long(0) * nrhs + rhs) * nblk + blockIdx.x] = make_double2(a_re, a_im);
+        part[(long(1) * nrhs + rhs) * nblk + blockIdx.x] = make_double2(rr, 0.0);
+    }
+}
+
 // Outer (FP64) steps.
 // r = b - Ax (tmp holds A x), partial |r|^2 into part (slot 0).
 __global__ void lp_resid_kernel(const double2* __restrict__ b, const double2* __restrict__ Ax,
@@ -1542,6 +1642,10 @@ struct LpNet
     double* s_part = nullptr;
     double* s_val = nullptr;    // per-rhs scalars [4][nrhs]
     BsState* s_state = nullptr;
+    // captured inner iterations of the solve (replayed per chunk) and its key
+    cudaGraphExec_t g_exec = nullptr;
+    std::vector<uintptr_t> g_key;
+    size_t g_nodes = 0;
     // solver settings
     double inner_tol = 1e-4;
     int inner_max = 400;
@@ -1579,10 +1683,12 @@ int set_conv_smem(dwf_ctx* c)
     CK(cudaFuncSetAttribute(lp_conv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_conv_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_conv_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_conv_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_conv_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_conv_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(lp_tc_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_tc_kernel<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     done_dev = c->device;
@@ -1715,6 +1821,7 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
         {
         case 16: lp_tc_kernel<16><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
         case 32: lp_tc_kernel<32><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
+        case 48: lp_tc_kernel<48><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
         case 64: lp_tc_kernel<64><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
         case 96: lp_tc_kernel<96><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
         default: return ctx_fail(c, DWF_BAD_ARG, "learned: unsupported channel count");
@@ -1752,6 +1859,7 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
     case 1: lp_conv_kernel<1><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
     case 2: lp_conv_kernel<2><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
     case 4: lp_conv_kernel<4><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
+    case 6: lp_conv_kernel<6><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
     case 8: lp_conv_kernel<8><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
     case 12: lp_conv_kernel<12><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
     default: return ctx_fail(c, DWF_BAD_ARG, "learned: unsupported channel count");
@@ -1785,7 +1893,7 @@ int lp_ensure_act(dwf_ctx* c, int nrhs)
 // hid[0], hid[1]; with `keep`, the layer inputs are also kept in act[] (act[0]
 // is `in` itself).
 int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* in, float2* out,
-           bool keep)
+           bool keep, bool planar_ready = false)
 {
     LpNet* n = c->lp;
     ST(lp_ensure_act(c, nrhs));
@@ -1800,9 +1908,12 @@ int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* 
         const int cin0 = adjoint ? n->cout[l0] : n->cin[l0];
         const int planes0 = cpad_of(cin0) / 4;
         const long np = long(nrhs) * planes0 * c->L.V;
-        lp_to_planar_kernel<<<grid_for(np, c->nsm), 256, 0, c->stream>>>(in, lop, cin0, planes0, c->L.V,
-                                                                          nrhs, n->hb[0]);
-        c->launches += 1;
+        if (!planar_ready)
+        {
+            lp_to_planar_kernel<<<grid_for(np, c->nsm), 256, 0, c->stream>>>(in, lop, cin0, planes0, c->L.V,
+                                                                              nrhs, n->hb[0]);
+            c->launches += 1;
+        }
         for (int s = 0; s < kLpLayers; ++s)
         {
             const int l = adjoint ? kLpLayers - 1 - s : s;
@@ -1826,6 +1937,15 @@ int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* 
         lcur = lh;
     }
     return DWF_OK;
+}
+
+// Whether lp_net runs the tcgen05 chain with BF16 planar activations.
+bool lp_chain(const dwf_ctx* c, bool adjoint)
+{
+    bool chain = c->lp->variant != 0;
+    for (int l = 0; l < kLpLayers; ++l)
+        chain = chain && tc_fits(c, l, adjoint);
+    return chain;
 }
 
 int lp_ensure_lpart(dwf_ctx* c, size_t n)
@@ -1989,6 +2109,8 @@ void lp_destroy(dwf_ctx* c)
     for (float2* b : n->s_f32)
         if (b)
             cudaFree(b);
+    if (n->g_exec)
+        cudaGraphExecDestroy(n->g_exec);
     delete n;
     c->lp = nullptr;
 }
@@ -2008,6 +2130,9 @@ int lp_solve(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double
     ST(lp_conf(c, nrhs, conf_h, &conf_d));
     ST(lp_transports(c));
     ST(lp_ensure_solver(c, nrhs));
+    // the fused update kernels write the network's planar input (hb[0]) before
+    // the network runs: size the activation buffers for this batch first
+    ST(lp_ensure_act(c, nrhs));
     const long fs = c->fsz();
     const long nf = fs * nrhs;
     const int nblk = int(std::min<long>(64, (fs + 4095) / 4096));
@@ -2083,37 +2208,97 @@ int lp_solve(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double
         lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, r}, Dot{r, r}, Dot{r, r}, 2, fs, nblk, n->s_part2);
         lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(0, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
         c->launches += 3;
-        const int chunk = 4;
-        for (int it = 0; it < n->inner_max; it += chunk)
-        {
-            for (int u = 0; u < chunk; ++u)
+        // one BiCGStab iteration; the coefficient kernels read the dot products
+        // of the previous kernel (slots 0, 1 of s_part2)
+        const bool chain = lp_chain(c, false);
+        const int planes0 = cpad_of(n->C0) / 4;
+        const int pgrid = grid_for(long(nrhs) * planes0 * c->L.V, c->nsm);
+        auto body = [&]() -> int {
+            lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(1, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+            if (chain)
             {
-                if (it + u > 0)
-                {
-                    lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, r}, Dot{r, r}, Dot{r, r}, 2, fs, nblk, n->s_part2);
-                    lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(1, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
-                    c->launches += 2;
-                }
-                else
-                {
-                    // first iteration: beta = 0, p = r
-                    lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(1, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
-                    c->launches += 1;
-                }
+                lp_bs_planar_kernel<<<pgrid, 256, 0, c->stream>>>(0, c->L.Ls, c->L.V, planes0, nrhs, n->s_state, p, r,
+                                                                  v, s, n->hb[0]);
+                ST(lp_net(c, false, nrhs, conf_d, p, ph, false, true));
+            }
+            else
+            {
                 lp_bs_vec_kernel<<<vgrid, 256, 0, c->stream>>>(0, fs, nrhs, n->s_state, p, r, v, s, x32, ph, sh, t, r);
                 ST(lp_net(c, false, nrhs, conf_d, p, ph, false));
-                ST(apply_dev(c, DWF_OP_D, nrhs, conf_d, 0, ph, v, 32));
-                lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, v}, Dot{rh, v}, Dot{rh, v}, 1, fs, nblk, n->s_part2);
-                lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(2, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+            }
+            ST(apply_dev(c, DWF_OP_D, nrhs, conf_d, 0, ph, v, 32));
+            lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{rh, v}, Dot{rh, v}, Dot{rh, v}, 1, fs, nblk, n->s_part2);
+            lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(2, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+            if (chain)
+            {
+                lp_bs_planar_kernel<<<pgrid, 256, 0, c->stream>>>(1, c->L.Ls, c->L.V, planes0, nrhs, n->s_state, p, r,
+                                                                  v, s, n->hb[0]);
+                ST(lp_net(c, false, nrhs, conf_d, s, sh, false, true));
+            }
+            else
+            {
                 lp_bs_vec_kernel<<<vgrid, 256, 0, c->stream>>>(1, fs, nrhs, n->s_state, p, r, v, s, x32, ph, sh, t, r);
                 ST(lp_net(c, false, nrhs, conf_d, s, sh, false));
-                ST(apply_dev(c, DWF_OP_D, nrhs, conf_d, 0, sh, t, 32));
-                lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{t, s}, Dot{t, t}, Dot{t, t}, 2, fs, nblk, n->s_part2);
-                lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(3, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
-                lp_bs_vec_kernel<<<vgrid, 256, 0, c->stream>>>(2, fs, nrhs, n->s_state, p, r, v, s, x32, ph, sh, t, r);
-                c->launches += 7;
             }
+            ST(apply_dev(c, DWF_OP_D, nrhs, conf_d, 0, sh, t, 32));
+            lp_dots_kernel<<<rgrid, 256, 0, c->stream>>>(Dot{t, s}, Dot{t, t}, Dot{t, t}, 2, fs, nblk, n->s_part2);
+            lp_bs_coef_kernel<<<sgrid, 128, 0, c->stream>>>(3, n->s_part2, nrhs, nblk, n->s_state, tgt2, n->inner_max);
+            lp_bs_xr_kernel<<<rgrid, 256, 0, c->stream>>>(fs, nblk, n->s_state, x32, ph, sh, s, t, r, rh, n->s_part2);
+            c->launches += 8;
             CK(cudaGetLastError());
+            return DWF_OK;
+        };
+        const int chunk = 4;
+        // the chunk of iterations is captured once into a CUDA graph and replayed;
+        // the first chunk runs directly (it also settles the Dslash autotuner)
+        const std::vector<uintptr_t> key = {uintptr_t(nrhs), uintptr_t(chain), uintptr_t(n->s_rhs),
+                                            uintptr_t(n->act_rhs), uintptr_t(n->T), uintptr_t(conf_d),
+                                            uintptr_t(c->U32), uintptr_t(n->variant),
+                                            uintptr_t(std::llround(std::log10(tgt2) * 1000.0)),
+                                            uintptr_t(n->inner_max), uintptr_t(nblk), uintptr_t(c->dslash_variant)};
+        for (int it = 0; it < n->inner_max; it += chunk)
+        {
+            if (it > 0 && n->g_exec && n->g_key == key)
+            {
+                CK(cudaGraphLaunch(n->g_exec, c->stream));
+                c->launches += n->g_nodes;
+            }
+            else if (it > 0)
+            {
+                if (n->g_exec)
+                {
+                    cudaGraphExecDestroy(n->g_exec);
+                    n->g_exec = nullptr;
+                }
+                const uint64_t l0 = c->launches;
+                CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                int st = DWF_OK;
+                for (int u = 0; u < chunk && st == DWF_OK; ++u)
+                    st = body();
+                cudaGraph_t g = nullptr;
+                const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+                if (st != DWF_OK || e != cudaSuccess)
+                {
+                    if (g)
+                        cudaGraphDestroy(g);
+                    return st != DWF_OK ? st : ctx_fail(c, DWF_CUDA_ERROR, "learned: graph capture failed");
+                }
+                const cudaError_t e2 = cudaGraphInstantiate(&n->g_exec, g, 0);
+                cudaGraphDestroy(g);
+                if (e2 != cudaSuccess)
+                {
+                    n->g_exec = nullptr;
+                    return ctx_fail(c, DWF_CUDA_ERROR, "learned: graph instantiation failed");
+                }
+                n->g_key = key;
+                n->g_nodes = c->launches - l0;
+                CK(cudaGraphLaunch(n->g_exec, c->stream));
+            }
+            else
+            {
+                for (int u = 0; u < chunk; ++u)
+                    ST(body());
+            }
             CK(cudaMemcpyAsync(hs.data(), n->s_state, nrhs * sizeof(BsState), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
             bool any = false;
@@ -2192,8 +2377,8 @@ int dwf_lp_init(dwf_ctx* c, int hidden, uint64_t seed)
 {
     if (!c)
         return DWF_BAD_ARG;
-    if (hidden != 8 && hidden != 16 && hidden != 32)
-        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: hidden must be 8, 16 or 32");
+    if (hidden != 8 && hidden != 16 && hidden != 24 && hidden != 32)
+        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: hidden must be 8, 16, 24 or 32");
     const int C0 = 2 * c->L.Ls;
     if (C0 > 48 || C0 * hidden > kGradThreads * kGradMaxPer)
         return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: 2*Ls*hidden must be <= 1024 and Ls <= 24");

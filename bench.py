@@ -3,8 +3,9 @@
 residual of 1e-10 on one B200, and the standalone Dslash bandwidth.
 
 Workload (one "step"): the per-configuration propagator set of the
-domain-wall analyzer on a 64x64 lattice, Ls = 16, M5 = 1.0, m_f = 0.05 with a
-seeded hot-start gauge field (theta uniform in [-pi, pi)): 2 spins x 4 source
+domain-wall analyzer on a 64x64 lattice, Ls = 16, M5 = 1.0, m_f = 0.05 on a
+seeded beta = 3.0 gauge configuration (pure-gauge plaquette distribution,
+three_part_dwf_study_b200.ensemble): 2 spins x 4 source
 times boundary point sources, 16 complex Z4 boundary-noise sources and
 2 spins x 2 source times boundary wall sources (28 right-hand sides), each
 solved as x = (D^dag D)^-1 D^dag src (domain_wall/include/correlator.hpp
@@ -14,7 +15,10 @@ equation is <= 1e-10.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One JSON line on rank 0. `value` = right-hand sides solved per second across
-all ranks, inputs resident in HBM, CUDA-event device time, max over ranks;
+all ranks by the fastest of the solvers measured (even-odd mixed CG, or the
+learned-preconditioned mixed BiCGStab, whose network is trained on four
+other configurations of the same ensemble; training time reported apart),
+inputs resident in HBM, CUDA-event device time, max over ranks;
 `e2e` = the same through the host C-ABI entry (dwf_set_gauge + dwf_propagators
 from pinned host buffers, solutions read back). With --gpus N (torchrun) every
 rank solves its own configuration's set (weak scaling, no exchange).
@@ -54,8 +58,18 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 def workload_gauge(rank):
-    rng = np.random.default_rng(GAUGE_SEED + 7919 * rank)
-    return rng.uniform(-np.pi, np.pi, 2 * NT * NX)
+    from three_part_dwf_study_b200.ensemble import quenched_theta
+    return quenched_theta(np.random.default_rng(GAUGE_SEED + 7919 * rank), NT, NX, BETA)
+
+
+def training_gauges(rank):
+    from three_part_dwf_study_b200.ensemble import quenched_ensemble
+    return quenched_ensemble(GAUGE_SEED + 1000003 + 7919 * rank, 4, NT, NX, BETA)
+
+
+LP_HIDDEN = 32
+LP_TRAIN = dict(steps=4000, batch=8, lr=3e-3, lr_decay_steps=1333, pairs_per_conf=32,
+                solver_iters=50, solver_every=2, solver_maxiter=20000, seed=11)
 
 
 def fi(s, t, x, a):
@@ -93,6 +107,19 @@ def workload_sources(rank):
                 v[LS - 1, t, :, 0] = 1.0
             srcs.append(v.ravel())
     return np.stack(srcs)
+
+
+def measured_tensor_peak():
+    """Measured dense BF16 TFLOP/s (burst) of this pool, else the fallback."""
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            v = json.loads(p.read_text()).get("bf16_tflops")
+            if v:
+                return float(v)
+        except (ValueError, OSError):
+            pass
+    return 1590.0
 
 
 def measured_peaks():
@@ -310,7 +337,7 @@ def impl_reference(args):
 
 def workload_config(solver):
     return {
-        "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, seeded hot "
+        "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, seeded beta=3.0 "
                      f"start, 28 boundary sources per step (8 point, 16 Z4 noise, 4 wall), "
                      f"to FP64 true residual {RTOL:g} of D^dag D"),
         "lattice": [NT, NX, LS], "rhs_per_step": 28, "rtol": RTOL, "solver": solver,
@@ -381,14 +408,31 @@ def impl_ours(args):
         return d.propagators_dev(src_dev, x_dev, rtol=RTOL, maxiter=MAXITER,
                                  solver=T.SOLVER_CG64)
 
+    def step_learned():
+        return d.propagators_dev(src_dev, x_dev, rtol=RTOL, maxiter=MAXITER,
+                                 solver=T.SOLVER_LEARNED)
+
+    # learned preconditioner: trained on four other configurations of the
+    # ensemble (training time reported apart), then used on the workload one
+    d.set_gauge(training_gauges(rank))
+    d.lp_init(hidden=LP_HIDDEN, seed=5 + rank)
+    torch.cuda.synchronize(dev)
+    tt0 = time.perf_counter()
+    train_info = d.lp_train(**LP_TRAIN)
+    torch.cuda.synchronize(dev)
+    train_s = time.perf_counter() - tt0
+    d.set_gauge(theta)
+
     with ClockSampler(local) as clk:
-        t_mixed, infos_m, kern_s, nkern, launches = timed(step_eo, args.steps, args.warmup, 1)
+        t_mixed, infos_m, kern_s, nkern, launches_eo = timed(step_eo, args.steps, args.warmup, 1)
+        t_learn, infos_l, _, _, launches_l = timed(step_learned, args.steps, args.warmup, 0)
     clocks = clk.summary()
     n_side = max(1, args.steps // 2)
     t_fp64, infos_f, kern64_s, nkern64, _ = timed(step_fp64, n_side, 1, 0)
     t_full, infos_full, _, _, _ = timed(step_mixed, n_side, 1, 0)
+    net_ms, net_flops = d.lp_time_network(nrhs, 10)
 
-    for infos in infos_m + infos_f + infos_full:
+    for infos in infos_m + infos_f + infos_full + infos_l:
         for i in infos:
             if not i["converged"] or i["true_relres"] > RTOL * 1.0001:
                 raise SystemExit(f"solve did not reach the FP64 true residual: {i}")
@@ -402,11 +446,20 @@ def impl_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    t_mixed_max = allmax(t_mixed)
+    t_eo_max = allmax(t_mixed)
+    t_learn_max = allmax(t_learn)
     t_fp64_max = allmax(t_fp64)
-    value = ws * nrhs * args.steps / t_mixed_max
+    eo_value = ws * nrhs * args.steps / t_eo_max
+    learned_value = ws * nrhs * args.steps / t_learn_max
     fp64_value = ws * nrhs * n_side / t_fp64_max
     full_value = ws * nrhs * n_side / allmax(t_full)
+    # the headline is the faster solver (decided by the max-over-ranks times,
+    # identical on every rank)
+    use_learned = learned_value > eo_value
+    value = learned_value if use_learned else eo_value
+    t_mixed_max = t_learn_max if use_learned else t_eo_max
+    launches = launches_l if use_learned else launches_eo
+    head_solver = T.SOLVER_LEARNED if use_learned else T.SOLVER_EO_MIXED
 
     # ---- end to end through the host C ABI ----
     src_host = torch.from_numpy(srcs.view(np.float64).copy()).pin_memory()
@@ -424,7 +477,7 @@ def impl_ours(args):
         infos = (A.SolveInfo * nrhs)()
         A.check(A.lib().dwf_propagators(d.handle, nrhs, None, C.c_void_p(src_np.ctypes.data),
                                         C.c_void_p(x_np.ctypes.data), RTOL, MAXITER,
-                                        T.SOLVER_EO_MIXED, infos), d.handle)
+                                        head_solver, infos), d.handle)
         return infos
 
     for _ in range(args.warmup):
@@ -492,18 +545,52 @@ def impl_ours(args):
                 "kernel_ms_per_launch": kernel_launch_s * 1e3,
                 "kernel_share_of_step": kern_s / t_mixed}
 
+    if use_learned:
+        # the dominant kernel is then the tensor-core network layer
+        tpeak = measured_tensor_peak()
+        ach = net_flops / (net_ms * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "achieved": round(ach, 1), "peak": tpeak, "unit": "TFLOP/s",
+                    "frac": round(ach / tpeak, 4), "traffic": None,
+                    "kernel": "lp_tc_kernel (4 launches per network application)",
+                    "peak_kind": "measured bf16_tflops (burst)",
+                    "alg_flops_per_application": net_flops,
+                    "kernel_ms_per_application": net_ms}
+
     line = {
         "metric": "dwf_propagator_solves_per_s_true_res_1e-10",
         "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_mixed_max / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+f64 (FP32 inner CG, FP64 reliable updates and true residual)",
-        "data": "synthetic (seeded hot-start links, boundary point/Z4/wall sources)",
-        "config": dict(workload_config("even-odd Schur mixed FP32/FP64 CG, then the full "
-                                       "D^dag D check"),
-                       parallelism=f"dp{ws} (independent configurations per rank)"),
+        "dtype": ("bf16 network + f32 BiCGStab + f64 defect correction" if use_learned else
+                  "f32+f64 (FP32 inner CG, FP64 reliable updates and true residual)"),
+        "data": "synthetic (seeded beta=3.0 pure-gauge configurations, boundary point/Z4/wall sources)",
+        "config": dict(workload_config(
+            "learned-preconditioned mixed BiCGStab (FP64 defect correction)" if use_learned else
+            "even-odd Schur mixed FP32/FP64 CG, then the full D^dag D check"),
+            parallelism=f"dp{ws} (independent configurations per rank)"),
+        "even_odd_mixed_cg": {"value": eo_value, "unit": "solves/s",
+                              "speedup_vs_plain_fp64": eo_value / fp64_value},
+        "learned_mixed": {
+            "value": learned_value, "unit": "solves/s",
+            "speedup_vs_plain_fp64": learned_value / fp64_value,
+            "bicgstab_iterations_mean": statistics.mean(
+                i["schur_iterations"] for infos in infos_l for i in infos),
+            "operator_applications_mean": statistics.mean(
+                2 * i["schur_iterations"] for infos in infos_l for i in infos),
+            "fallbacks": sum(i["fallback"] for infos in infos_l for i in infos),
+            "defect_corrections_mean": statistics.mean(
+                i["reliable_updates"] for infos in infos_l for i in infos),
+            "network": {"hidden": LP_HIDDEN, "layers": 4, "stencil": "3x3 parallel-transported",
+                        "ms_per_application": net_ms,
+                        "tflops": net_flops / (net_ms * 1e-3) / 1e12,
+                        "frac_of_bf16_peak": (net_flops / (net_ms * 1e-3) / 1e12) /
+                        measured_tensor_peak()},
+            "training": dict(train_info, wall_seconds=train_s, configurations=4,
+                             settings=LP_TRAIN)},
         "plain_fp64_cg": {"value": fp64_value, "unit": "solves/s",
                           "speedup_of_value": value / fp64_value,
+                          "operator_applications_mean": statistics.mean(
+                              2 * i["iterations"] for infos in infos_f for i in infos),
                           "iterations_mean": statistics.mean(
                               i["iterations"] for infos in infos_f for i in infos)},
         "mixed_full_lattice_cg": {"value": full_value, "unit": "solves/s",

@@ -409,6 +409,10 @@ typedef struct
  * of every step. */
 int dwf_lp_train(dwf_ctx* ctx, const dwf_lp_train_params* params, dwf_lp_train_info* info,
                  double* history);
+/* Device time of one network application to nrhs Gaussian fields (CUDA
+ * events around `reps` back-to-back applications on the context stream) and
+ * its arithmetic: 8 * 9 * sum_l cin_l cout_l * V * nrhs real flops. */
+int dwf_lp_time_network(dwf_ctx* ctx, int nrhs, int reps, double* ms_per_apply, double* flops_per_apply);
 /* Layer kernel: -1 automatic (default: the tcgen05 kernel wherever its shared-
  * memory tile fits, else the mma.sync kernel), 0 the mma.sync kernel, 1 the
  * tcgen05 kernel only (DWF_BAD_ARG where it does not fit). */

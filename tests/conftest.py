@@ -53,17 +53,6 @@ def random_field(rng, n):
 
 
 def quenched_theta(rng, nt, nx, beta):
-    """Seeded 2-D U(1) gauge field with plaquette angles drawn independently
-    from exp(beta cos P) (built in an axial gauge, then gauge-randomised);
-    the periodic closure leaves one plaquette per slice off that law."""
-    P = rng.vonmises(0.0, beta, size=(nt, nx))
-    th = np.zeros((2, nt, nx))
-    th[1, 0] = rng.uniform(-np.pi, np.pi, nx)
-    for t in range(nt - 1):
-        th[1, t + 1] = th[1, t] + P[t]
-    for x in range(nx - 1):
-        th[0, nt - 1, x + 1] = th[0, nt - 1, x] + th[1, 0, x] - th[1, nt - 1, x] - P[nt - 1, x]
-    phi = rng.uniform(-np.pi, np.pi, (nt, nx))
-    th[0] += phi - np.roll(phi, -1, 0)
-    th[1] += phi - np.roll(phi, -1, 1)
-    return np.angle(np.exp(1j * th)).ravel()
+    """Seeded pure-gauge configuration (see three_part_dwf_study_b200.ensemble)."""
+    from three_part_dwf_study_b200.ensemble import quenched_theta as q
+    return q(rng, nt, nx, beta)

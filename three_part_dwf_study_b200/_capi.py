@@ -135,6 +135,7 @@ SIGNATURES = {
     "dwf_lp_train": (_I, [_P, C.POINTER(LpTrainParams), C.POINTER(LpTrainInfo), _P]),
     "dwf_lp_set_solver": (_I, [_P, _D, _I, _I]),
     "dwf_lp_set_variant": (_I, [_P, _I]),
+    "dwf_lp_time_network": (_I, [_P, _I, _I, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
 _lib = None

@@ -2665,6 +2665,43 @@ int dwf_lp_train(dwf_ctx* c, const dwf_lp_train_params* tp, dwf_lp_train_info* t
     return DWF_OK;
 }
 
+int dwf_lp_time_network(dwf_ctx* c, int nrhs, int reps, double* ms_per_apply, double* flops_per_apply)
+{
+    if (!c || !c->lp || nrhs < 1 || nrhs > 65535 || reps < 1 || !ms_per_apply)
+        return c ? ctx_fail(c, DWF_BAD_ARG, "dwf_lp_time_network: bad arguments or no network") : DWF_BAD_ARG;
+    if (c->nconf < 1)
+        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_time_network: no gauge configuration");
+    CK(cudaSetDevice(c->device));
+    LpNet* n = c->lp;
+    const int* conf_d = nullptr;
+    ST(lp_conf(c, nrhs, nullptr, &conf_d));
+    ST(lp_transports(c));
+    ST(lp_ensure_solver(c, nrhs));
+    ST(lp_ensure_act(c, nrhs));
+    const long nf = long(nrhs) * c->fsz();
+    ST(lp_gauss(c, n->s_r64, nf, 12345));
+    lp_f64_to_f32_kernel<<<grid_for(nf, c->nsm), 256, 0, c->stream>>>(n->s_r64, n->s_f32[0], nf);
+    c->launches += 1;
+    ST(lp_net(c, false, nrhs, conf_d, n->s_f32[0], n->s_f32[1], false));  // warm-up
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < reps; ++r)
+        ST(lp_net(c, false, nrhs, conf_d, n->s_f32[0], n->s_f32[1], false));
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *ms_per_apply = double(ms) / reps;
+    if (flops_per_apply)
+    {
+        double cc = 0.0;
+        for (int l = 0; l < kLpLayers; ++l)
+            cc += double(n->cin[l]) * n->cout[l];
+        // 9 offsets, complex multiply-add = 8 real flops
+        *flops_per_apply = 8.0 * 9.0 * cc * double(c->L.V) * nrhs;
+    }
+    return lp_check_err(c);
+}
+
 int dwf_lp_set_variant(dwf_ctx* c, int variant)
 {
     if (!c || !c->lp || variant < -1 || variant > 1)

@@ -117,6 +117,13 @@ class LearnedMixin:
                                          _ptr(h) if h is not None else None))
         return (info.as_dict(), h) if history else info.as_dict()
 
+    def lp_time_network(self, nrhs, reps=10):
+        """(ms per network application, flops per application) on nrhs fields."""
+        ms = C.c_double()
+        fl = C.c_double()
+        self._check(A.lib().dwf_lp_time_network(self._h, int(nrhs), int(reps), C.byref(ms), C.byref(fl)))
+        return ms.value, fl.value
+
     def lp_set_variant(self, variant):
         """Layer kernel: -1 automatic, 0 mma.sync, 1 tcgen05."""
         self._check(A.lib().dwf_lp_set_variant(self._h, int(variant)))

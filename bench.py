@@ -658,6 +658,31 @@ def profile_case():
     return 0
 
 
+def profile_learned():
+    """A short training run on the training configurations, then (inside the
+    NVTX range "learned") one learned propagator batch of the workload and
+    three network applications on 28 fields (for ncu launch lists and captures
+    of the network layer kernel)."""
+    import torch
+    import three_part_dwf_study_b200 as T
+    d = T.DomainWall(NT, NX, LS, M5, MF, BETA)
+    d.set_gauge(training_gauges(0))
+    d.lp_init(hidden=LP_HIDDEN, seed=5)
+    d.lp_train(**dict(LP_TRAIN, steps=400))
+    d.set_gauge(workload_gauge(0))
+    src = torch.from_numpy(workload_sources(0).view(np.float64).copy()).cuda()
+    x = torch.zeros_like(src)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("learned")
+    infos = d.propagators_dev(src, x, rtol=RTOL, maxiter=MAXITER, solver=T.SOLVER_LEARNED)
+    d.lp_time_network(src.shape[0], 3)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    assert all(i["converged"] for i in infos)
+    d.close()
+    return 0
+
+
 def profile_dslash():
     """Two applications of D at the Dslash bench lattice for each kernel
     variant and precision (for ncu)."""
@@ -689,11 +714,14 @@ def main():
     ap.add_argument("--calibrate-reference", action="store_true")
     ap.add_argument("--profile-case", action="store_true")
     ap.add_argument("--profile-dslash", action="store_true")
+    ap.add_argument("--profile-learned", action="store_true")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
     if args.profile_dslash:
         return profile_dslash()
+    if args.profile_learned:
+        return profile_learned()
     if args.calibrate_reference:
         return calibrate_reference()
     if args.warmup < 3 and args.impl == "ours":

@@ -3,8 +3,10 @@ headers (three_part_dwf_study_b200/host/dropin) so that every hot-path call
 runs on the GPU through libdwfb200.so, reproduce the reference's own runs
 (tests/golden/dwf_hmc_8x8x4, wil_hmc_8x8): same accept decisions and
 configurations (1e-9 relative), same CSV outputs (6 significant digits, 2e-5).
-Both solver paths are exercised: DWF_B200_SOLVER=cg64 (the reference's FP64
-CG) and the default mixed FP32/FP64 path."""
+Three solver settings are exercised: DWF_B200_SOLVER=cg64 (the reference's
+FP64 CG everywhere), =mixed (the full-lattice mixed FP32/FP64 CG everywhere)
+and the default (mixed CG in HMC, even-odd Schur mixed CG for the analyzers'
+propagators)."""
 import csv
 import os
 import shutil
@@ -35,7 +37,7 @@ def table(path):
     return np.array([[float(v) for v in r.values()] for r in rows])
 
 
-@pytest.mark.parametrize("solver", ["cg64", "mixed"])
+@pytest.mark.parametrize("solver", ["cg64", "mixed", "default"])
 def test_dropin_domain_wall_generate_and_analyze(golden, tmp_path, solver):
     g = golden("dwf_hmc_8x8x4")
     shutil.copy2(g.dir / "parameters.txt", tmp_path / "parameters.txt")
@@ -55,7 +57,7 @@ def test_dropin_domain_wall_generate_and_analyze(golden, tmp_path, solver):
         assert np.allclose(a, b, rtol=2e-5, atol=1e-12 * np.abs(b).max()), name
 
 
-@pytest.mark.parametrize("solver", ["cg64", "mixed"])
+@pytest.mark.parametrize("solver", ["cg64", "mixed", "default"])
 def test_dropin_wilson_generate_and_analyze(golden, tmp_path, solver):
     g = golden("wil_hmc_8x8")
     shutil.copy2(g.dir / "parameters.txt", tmp_path / "parameters.txt")

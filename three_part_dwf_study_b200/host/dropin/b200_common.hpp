@@ -1,6 +1,9 @@
 // Shared helpers of the drop-in headers: status-to-exception mapping and the
-// solver path (DWF_B200_SOLVER=cg64 selects the reference FP64 CG, anything
-// else the mixed FP32/FP64 reliable-update CG; both meet the same rtol).
+// solver path. DWF_B200_SOLVER=cg64 selects the reference FP64 CG everywhere;
+// =mixed the full-lattice mixed FP32/FP64 reliable-update CG everywhere;
+// otherwise (default) HMC solves use the mixed CG and propagator solves the
+// even-odd Schur mixed CG (which ends with the full D^dag D check). All meet
+// the same rtol on the FP64 true residual.
 #pragma once
 
 #include <complex>
@@ -18,6 +21,20 @@ inline int solver()
     static const int s = [] {
         const char* v = std::getenv("DWF_B200_SOLVER");
         return (v && std::strcmp(v, "cg64") == 0) ? DWF_SOLVER_CG64 : DWF_SOLVER_MIXED;
+    }();
+    return s;
+}
+
+// Solver of the propagator (CGNR) solves of the analyzers.
+inline int prop_solver()
+{
+    static const int s = [] {
+        const char* v = std::getenv("DWF_B200_SOLVER");
+        if (v && std::strcmp(v, "cg64") == 0)
+            return int(DWF_SOLVER_CG64);
+        if (v && std::strcmp(v, "mixed") == 0)
+            return int(DWF_SOLVER_MIXED);
+        return int(DWF_SOLVER_EO_MIXED);
     }();
     return s;
 }

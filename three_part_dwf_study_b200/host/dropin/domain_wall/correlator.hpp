@@ -31,7 +31,7 @@ inline ComplexCorr estimate_pseudoscalar_loop_density(const Gauge& theta, unsign
     std::vector<signed char> z4(static_cast<std::size_t>(eta_noise_vectors) * Nt * Nx * Ns);
     b200::check(c, dwf_z4_digits(seed, static_cast<long>(z4.size()), z4.data()));
     const dwf_measure_params mp{0, 0, eta_noise_vectors, 0, propagator_rtol, propagator_maxiter,
-                                b200::solver()};
+                                b200::prop_solver()};
     ComplexCorr loop(static_cast<std::size_t>(Nt) * Nx);
     std::vector<dwf_solve_info> info(eta_noise_vectors);
     b200::check(c, dwf_measure(c, &mp, 1, theta.data(), z4.data(), nullptr, nullptr,
@@ -48,7 +48,7 @@ inline std::vector<Corr> compute_momentum_CPP(const Gauge& theta)
         throw std::runtime_error("analysis.max_momentum is outside 0..Nx/2");
     dwf_ctx* c = b200_dwf_context();
     const dwf_measure_params mp{2, 0, 0, max_momentum, propagator_rtol, propagator_maxiter,
-                                b200::solver()};
+                                b200::prop_solver()};
     std::vector<double> mom(static_cast<std::size_t>(max_momentum + 1) * Nt);
     std::vector<dwf_solve_info> info(4);
     b200::check(c, dwf_measure(c, &mp, 1, theta.data(), nullptr, nullptr, nullptr, nullptr,
@@ -91,7 +91,7 @@ inline std::array<VectorC, 2> boundary_wall_source_propagator(const Gauge& theta
     dwf_solve_info info[2];
     b200::check(c, dwf_propagators(c, 2, nullptr, reinterpret_cast<const double*>(src.data()),
                                    reinterpret_cast<double*>(x.data()), propagator_rtol,
-                                   propagator_maxiter, b200::solver(), info));
+                                   propagator_maxiter, b200::prop_solver(), info));
     std::array<VectorC, 2> props;
     for (int b = 0; b < Ns; ++b)
     {
@@ -106,7 +106,7 @@ inline std::array<VectorC, 2> boundary_wall_source_propagator(const Gauge& theta
 inline CorrelatorPair compute_CPP_CJ5(const Gauge& theta)
 {
     dwf_ctx* c = b200_dwf_context();
-    const dwf_measure_params mp{0, 2, 0, 0, propagator_rtol, propagator_maxiter, b200::solver()};
+    const dwf_measure_params mp{0, 2, 0, 0, propagator_rtol, propagator_maxiter, b200::prop_solver()};
     CorrelatorPair out{Corr(Nt, 0.0), Corr(Nt, 0.0)};
     dwf_solve_info info[4];
     b200::check(c, dwf_measure(c, &mp, 1, theta.data(), nullptr, out.CPP.data(), out.CJ5.data(),

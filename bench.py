@@ -704,6 +704,40 @@ def profile_dslash():
     return 0
 
 
+def dslash_variants():
+    """Event-timed GB/s of both Dslash kernels (site, column) in FP64 and FP32
+    at 256x256x16 and 512x512x16 (one JSON line)."""
+    import torch
+    import three_part_dwf_study_b200 as T
+    from three_part_dwf_study_b200 import _capi as A
+    out = {}
+    for lat in ((256, 256, 16), DSLASH_LATTICE):
+        Dt, Dx, Dl = lat
+        d = T.DomainWall(Dt, Dx, Dl, M5, MF, BETA)
+        d.set_gauge(np.random.default_rng(3).uniform(-np.pi, np.pi, 2 * Dt * Dx))
+        st = torch.cuda.ExternalStream(d.stream_ptr())
+        for prec, dt, w in ((64, torch.float64, 8), (32, torch.float32, 4)):
+            a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
+            b = torch.empty_like(a)
+            for v, name in ((0, "site"), (1, "column")):
+                A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
+                for _ in range(3):
+                    d.apply_dev(0, a, b)
+                d.sync()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                for _ in range(20):
+                    d.apply_dev(0, a, b)
+                e1.record(st)
+                e1.synchronize()
+                tsec = e0.elapsed_time(e1) * 1e-3 / 20
+                out[f"{Dt}x{Dx}x{Dl}_fp{prec}_{name}"] = round(dslash_bytes(Dt * Dx, Dl, w) / tsec / 1e9, 1)
+        d.close()
+    print(json.dumps({"dslash_GBs": out, "bytes_rule": "V*(Ls*64+32) FP64, V*(Ls*32+16) FP32"}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -715,6 +749,7 @@ def main():
     ap.add_argument("--profile-case", action="store_true")
     ap.add_argument("--profile-dslash", action="store_true")
     ap.add_argument("--profile-learned", action="store_true")
+    ap.add_argument("--dslash-variants", action="store_true")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
@@ -722,6 +757,8 @@ def main():
         return profile_dslash()
     if args.profile_learned:
         return profile_learned()
+    if args.dslash_variants:
+        return dslash_variants()
     if args.calibrate_reference:
         return calibrate_reference()
     if args.warmup < 3 and args.impl == "ours":

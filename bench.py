@@ -335,6 +335,57 @@ def impl_reference(args):
     return 0
 
 
+HMC_EPS, HMC_STEPS = 0.01, 40  # the reference's dwf.epsilon and dwf.leapfrog_steps
+
+
+def hmc_compare(T, d, rank, ntraj):
+    """ntraj domain-wall HMC trajectories from the workload configuration, each
+    run twice from identical momenta and pseudofermion draws (libstdc++
+    streams, the reference's order: chi then pi): pseudofermion solves by the
+    plain FP64 CG and by the mixed CG, both to 1e-10. Reports device time per
+    trajectory (CUDA events on the library stream around the whole
+    trajectory), dH of each and their largest difference, and the plaquette."""
+    import torch
+    from three_part_dwf_study_b200.rng import Rng
+    if ntraj < 1:
+        return None
+    stream = torch.cuda.ExternalStream(d.stream_ptr())
+    theta = workload_gauge(rank)
+    rng = Rng(1234 + rank)
+    res = {"lattice": [NT, NX, LS], "epsilon": HMC_EPS, "leapfrog_steps": HMC_STEPS,
+           "rtol": RTOL, "trajectories": ntraj}
+    per = {T.SOLVER_CG64: [], T.SOLVER_MIXED: []}
+    dh = {T.SOLVER_CG64: [], T.SOLVER_MIXED: []}
+    plaq = []
+    for k in range(ntraj):
+        chi = rng.pseudofermion(d.Ndof)
+        mom = rng.normals(d.Ngauge)
+        outs = {}
+        for solver in (T.SOLVER_CG64, T.SOLVER_MIXED):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            out, info = d.hmc_trajectory(theta, chi, mom, HMC_EPS, HMC_STEPS, rtol=RTOL,
+                                         maxiter=MAXITER, solver=solver)
+            e1.record(stream)
+            e1.synchronize()
+            per[solver].append(e0.elapsed_time(e1) * 1e-3)
+            dh[solver].append(info["dH"])
+            outs[solver] = (out, info)
+        out, info = outs[T.SOLVER_CG64]
+        plaq.append(info["plaquette"])
+        if np.random.default_rng(k).uniform() < min(1.0, float(np.exp(-info["dH"]))):
+            theta = out
+    for solver, name in ((T.SOLVER_CG64, "plain_fp64_cg"), (T.SOLVER_MIXED, "mixed_cg")):
+        res[name] = {"seconds_per_trajectory": statistics.mean(per[solver]), "dH": dh[solver]}
+    res["max_abs_dH_difference"] = max(abs(a - b) for a, b in zip(dh[T.SOLVER_CG64], dh[T.SOLVER_MIXED]))
+    res["speedup_mixed_vs_fp64"] = res["plain_fp64_cg"]["seconds_per_trajectory"] / \
+        res["mixed_cg"]["seconds_per_trajectory"]
+    res["plaquette"] = plaq
+    return res
+
+
 def workload_config(solver):
     return {
         "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, seeded beta=3.0 "
@@ -527,6 +578,9 @@ def impl_ours(args):
     dslash["lattice"] = list(DSLASH_LATTICE)
     dslash["bytes_rule"] = "V*(Ls*64+32) B (FP64), V*(Ls*32+16) B (FP32) per application"
 
+    # ---- HMC on the same lattice: FP64 and mixed CG on the same trajectories ----
+    hmc = hmc_compare(T, d, rank, args.hmc_trajectories)
+
     # ---- roofline of the dominant kernel (the persistent even-odd solver) ----
     V = NT * NX
     iters = sum(i["schur_iterations"] for infos in infos_m for i in infos)
@@ -605,6 +659,7 @@ def impl_ours(args):
                 "agrees_with_device_run": e2e_agree},
         "roofline": roofline,
         "dslash": dslash,
+        "hmc": hmc,
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -746,6 +801,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
+    ap.add_argument("--hmc-trajectories", type=int, default=2,
+                    help="HMC trajectories compared between FP64 and mixed CG (0: skip)")
     ap.add_argument("--profile-case", action="store_true")
     ap.add_argument("--profile-dslash", action="store_true")
     ap.add_argument("--profile-learned", action="store_true")

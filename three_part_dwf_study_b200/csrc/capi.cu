@@ -290,6 +290,7 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     d.eigen_rule = eigen_rule;
     d.delta = 0.1;
     d.stall_limit = 3;
+    d.ru_period = mixed ? kRuPeriod : 1;
     d.out_iters = c->w_iters;
     d.out_relres = c->w_relres;
     d.out_status = c->w_status;

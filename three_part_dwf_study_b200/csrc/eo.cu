@@ -261,9 +261,10 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
             s.rr[j] = rn;
         }
         __syncthreads();
-        const int nru = compact(d.nrhs, s.act, s.scratch, [&](int j) {
+        const bool ru_now = d.ru_period <= 1 || it % d.ru_period == 0 || it == d.maxiter;
+        const int nru = ru_now ? compact(d.nrhs, s.act, s.scratch, [&](int j) {
             return s.state[j] == RHS_ACTIVE && (s.flag[j] & 1);
-        });
+        }) : 0;
         if (nru > 0)
         {
             // FP64 residual of the Schur normal equation at x + e:

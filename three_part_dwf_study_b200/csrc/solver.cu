@@ -234,9 +234,10 @@ __global__ void __launch_bounds__(256, MINB) cg_mixed_kernel(SolveDesc d)
             s.rr[j] = rn;
         }
         __syncthreads();
-        const int nru = compact(d.nrhs, s.act, s.scratch, [&](int j) {
+        const bool ru_now = d.ru_period <= 1 || it % d.ru_period == 0 || it == d.maxiter;
+        const int nru = ru_now ? compact(d.nrhs, s.act, s.scratch, [&](int j) {
             return s.state[j] == RHS_ACTIVE && (s.flag[j] & 1);
-        });
+        }) : 0;
         if (nru > 0)
         {
             // Reliable update, part 1: t = D1 (x + e) in FP64, with x + e

@@ -41,6 +41,11 @@ struct SolveDesc
     int eigen_rule;   // stop at |r|^2 < tol^2 |b|^2 and count as Eigen's ConjugateGradient
     double delta;     // reliable-update trigger: |r32| < delta * |r| at the last update
     int stall_limit;  // consecutive non-improving reliable updates before giving up
+    // reliable updates run only at iterations divisible by ru_period (and at
+    // maxiter), so that the right-hand sides of a batch that want one share the
+    // FP64 phases instead of each paying them at its own iteration (0 or 1:
+    // every iteration)
+    int ru_period;
     // outputs (device, [nrhs])
     int* out_iters;
     double* out_relres;
@@ -50,6 +55,12 @@ struct SolveDesc
     unsigned long long timeout_ns;
     unsigned expected_blocks;  // normally gridDim.x
 };
+
+// Reliable-update period of the mixed solvers (iterations).
+#ifndef DWFB_RU_PERIOD
+#define DWFB_RU_PERIOD 8
+#endif
+constexpr int kRuPeriod = DWFB_RU_PERIOD;
 
 // Dynamic shared memory needed by the solver kernels for nrhs right-hand sides.
 inline size_t solver_smem_bytes(int nrhs)

@@ -21,16 +21,6 @@ namespace dwfb {
 
 using namespace persist;
 
-struct EoDesc
-{
-    SolveDesc d;   // fields are parity fields (fsz = 2*Vh*Ls); d.nch/d.ch chunk 5-D odd sites
-    EoGeo g;
-    int nch4, ch4;  // chunking of the 4-D even sites
-    double2* y64;   // even temporaries
-    float2* y32;
-    double2* xn64;  // reliable update: x + e parked here
-};
-
 namespace {
 
 constexpr int kEven = 0, kOdd = 1;
@@ -177,6 +167,11 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
     nact = compact(d.nrhs, s.act, s.scratch, [&](int j) { return s.state[j] == RHS_ACTIVE; });
     const int nsite4 = g.Vh, nsite5 = g.Vh * d.L.Ls;
     const long fh = fs;
+    // per-thread slice columns for the FP32 hop + M5^-1 phases (after the
+    // solver's own shared memory, 16-byte aligned)
+    extern __shared__ double sm_all[];
+    Spinor<float>* zs = reinterpret_cast<Spinor<float>*>(
+        reinterpret_cast<char*>(sm_all) + ((solver_smem_bytes(d.nrhs) + 15) & ~size_t(15))) + threadIdx.x;
 
     for (int it = 1; it <= d.maxiter && nact > 0; ++it)
     {
@@ -184,9 +179,14 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
         sweep_sites(d, s.act, nact, nsite4, e.nch4, e.ch4, s.scratch, false,
                     [&](int j, int h, long uo) {
                         const int t = h / g.Nxh, k = h - t * g.Nxh;
-                        eo_hopinv_site<false, float>(FieldLd<float>{d.p32 + j * fh}, true,
-                                                     nullptr, 1.0f, e.y32 + j * fh, d.U32 + uo,
-                                                     d.L, g, t, k, kEven);
+                        if (e.zsmem)
+                            eo_hopinv_site_smem<false, float>(FieldLd<float>{d.p32 + j * fh},
+                                                              e.y32 + j * fh, d.U32 + uo, d.L, g,
+                                                              t, k, kEven, zs, blockDim.x);
+                        else
+                            eo_hopinv_site<false, float>(FieldLd<float>{d.p32 + j * fh}, true,
+                                                         nullptr, 1.0f, e.y32 + j * fh,
+                                                         d.U32 + uo, d.L, g, t, k, kEven);
                         return make_double2(0.0, 0.0);
                     });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
@@ -222,9 +222,14 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
         sweep_sites(d, s.act, nact, nsite4, e.nch4, e.ch4, s.scratch, false,
                     [&](int j, int h, long uo) {
                         const int t = h / g.Nxh, k = h - t * g.Nxh;
-                        eo_hopinv_site<true, float>(FieldLd<float>{d.t32 + j * fh}, true, nullptr,
-                                                    1.0f, e.y32 + j * fh, d.U32 + uo, d.L, g, t,
-                                                    k, kEven);
+                        if (e.zsmem)
+                            eo_hopinv_site_smem<true, float>(FieldLd<float>{d.t32 + j * fh},
+                                                             e.y32 + j * fh, d.U32 + uo, d.L, g,
+                                                             t, k, kEven, zs, blockDim.x);
+                        else
+                            eo_hopinv_site<true, float>(FieldLd<float>{d.t32 + j * fh}, true,
+                                                        nullptr, 1.0f, e.y32 + j * fh, d.U32 + uo,
+                                                        d.L, g, t, k, kEven);
                         return make_double2(0.0, 0.0);
                     });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))

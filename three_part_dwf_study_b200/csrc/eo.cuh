@@ -23,12 +23,25 @@
 #pragma once
 
 #include "dirac.cuh"
+#include "solver.cuh"
 
 namespace dwfb {
 
 struct EoGeo
 {
     int Nxh, Vh;
+};
+
+// Launch descriptor of the persistent even-odd solver kernel.
+struct EoDesc
+{
+    SolveDesc d;    // fields are parity fields (fsz = 2*Vh*Ls); d.nch/d.ch chunk 5-D odd sites
+    EoGeo g;
+    int nch4, ch4;  // chunking of the 4-D even sites
+    double2* y64;   // even temporaries
+    float2* y32;
+    double2* xn64;  // reliable update: x + e parked here
+    int zsmem;      // 1: the FP32 hop + M5^-1 phases keep the slices in shared memory
 };
 
 // Hop term H (DAG = false) or H^dag of the site (s, t, x), reading the other
@@ -168,6 +181,66 @@ __device__ __forceinline__ void eo_hopinv_site(const Ld& in, bool has_in,
             out[i] = y;
         }
     }
+}
+
+// Same as eo_hopinv_site with the Ls slices of this thread's column kept in
+// shared memory (zs[s * zstride], this thread's own slots) while the two
+// recurrences run, so `out` is written once per slice instead of being read
+// and rewritten in the serial fifth-dimension sweeps.
+template <bool DAG, typename R, typename Ld>
+__device__ __forceinline__ void eo_hopinv_site_smem(const Ld& in, cplx<R>* __restrict__ out,
+                                                    const cplx<R>* __restrict__ U, const Lat& L,
+                                                    EoGeo g, int t, int k, int po,
+                                                    Spinor<R>* zs, int zstride)
+{
+    using T = cplx<R>;
+    const int x = 2 * k + ((t + po) & 1);
+    const int h = t * g.Nxh + k;
+    const int Ls = L.Ls;
+    const R c = R(L.diag), ci = R(1) / c, mf = R(L.mf);
+    T s_up = mkc(R(0), R(0)), s_dn = mkc(R(0), R(0));
+    R pw = ci;
+    R cmls = R(1);
+    for (int s = 0; s < Ls; ++s)
+    {
+        const Spinor<R> hv = eo_hop<DAG, R>(in, U, L, g, s, t, x);
+        zs[s * zstride] = hv;
+        const T zu = DAG ? hv.s0 : hv.s1;
+        const T zd = DAG ? hv.s1 : hv.s0;
+        s_up += pw * zu;
+        s_dn = ci * (s_dn + zd);
+        pw *= ci;
+        cmls *= ci;
+    }
+    const R den = R(1) / (R(1) + mf * cmls);
+    // up form (spin component DAG ? 0 : 1): y(Ls-1) from y(0), then downwards
+    {
+        const T y0 = den * s_up;
+        Spinor<R>& zl = zs[(Ls - 1) * zstride];
+        T y = ci * ((DAG ? zl.s0 : zl.s1) - mf * y0);
+        (DAG ? zl.s0 : zl.s1) = y;
+        for (int s = Ls - 2; s >= 0; --s)
+        {
+            Spinor<R>& z = zs[s * zstride];
+            y = ci * ((DAG ? z.s0 : z.s1) + y);
+            (DAG ? z.s0 : z.s1) = y;
+        }
+    }
+    // down form (the other component): y(0) from y(Ls-1), then upwards
+    {
+        const T yl = den * s_dn;
+        Spinor<R>& z0 = zs[0];
+        T y = ci * ((DAG ? z0.s1 : z0.s0) - mf * yl);
+        (DAG ? z0.s1 : z0.s0) = y;
+        for (int s = 1; s < Ls; ++s)
+        {
+            Spinor<R>& z = zs[s * zstride];
+            y = ci * ((DAG ? z.s1 : z.s0) + y);
+            (DAG ? z.s1 : z.s0) = y;
+        }
+    }
+    for (int s = 0; s < Ls; ++s)
+        st_spinor(out, long(s) * g.Vh + h, zs[s * zstride]);
 }
 
 // 5-D site (s, h) of parity q: a + M5 m - H y (M5^dag, H^dag when DAG); any

@@ -17,15 +17,6 @@ using namespace dwfb;
 
 namespace dwfb {
 
-struct EoDesc
-{
-    SolveDesc d;
-    EoGeo g;
-    int nch4, ch4;
-    double2* y64;
-    float2* y32;
-    double2* xn64;
-};
 __global__ void eo_pack_kernel(Lat L, EoGeo g, const double2* full, double2* ev, double2* od,
                                long nrhs);
 __global__ void eo_unpack_kernel(Lat L, EoGeo g, const double2* ev, const double2* od,
@@ -150,7 +141,20 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
         e.xn64 = c->eo_xn;
 
         const void* fn = reinterpret_cast<const void*>(&cg_eo_mixed_kernel);
-        const size_t smem = solver_smem_bytes(n);
+        // the FP32 hop + M5^-1 phases keep each thread's Ls slices in shared
+        // memory when that costs no resident blocks (registers bound them)
+        const size_t smem_base = solver_smem_bytes(n);
+        const size_t smem_z = ((smem_base + 15) & ~size_t(15)) + size_t(256) * c->L.Ls * sizeof(float4);
+        int bps_base = 0, bps_z = 0;
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_base)));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_base, fn, 256, smem_base));
+        if (smem_z <= size_t(200 * 1024))
+        {
+            CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_z)));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_z, fn, 256, smem_z));
+        }
+        e.zsmem = (bps_z >= bps_base && bps_z > 0) ? 1 : 0;
+        const size_t smem = e.zsmem ? smem_z : smem_base;
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         int bps = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, 256, smem));

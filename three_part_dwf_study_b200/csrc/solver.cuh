@@ -58,12 +58,12 @@ struct SolveDesc
 
 // Reliable-update period of the mixed solvers (iterations).
 #ifndef DWFB_RU_PERIOD
-#define DWFB_RU_PERIOD 8
+#define DWFB_RU_PERIOD 16
 #endif
 constexpr int kRuPeriod = DWFB_RU_PERIOD;
 
 // Dynamic shared memory needed by the solver kernels for nrhs right-hand sides.
-inline size_t solver_smem_bytes(int nrhs)
+__host__ __device__ inline size_t solver_smem_bytes(int nrhs)
 {
     return 64 * sizeof(double) + size_t(nrhs) * (6 * sizeof(double) + 5 * sizeof(int));
 }

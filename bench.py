@@ -759,6 +759,33 @@ def profile_dslash():
     return 0
 
 
+def eo_phases():
+    """Per-phase device time of the even-odd solver kernel on one propagator
+    batch of the workload (one JSON line, us per iteration)."""
+    import ctypes as C
+    import torch
+    import three_part_dwf_study_b200 as T
+    from three_part_dwf_study_b200 import _capi as A
+    d = T.DomainWall(NT, NX, LS, M5, MF, BETA)
+    d.set_gauge(workload_gauge(0))
+    src = torch.from_numpy(workload_sources(0).view(np.float64).copy()).cuda()
+    x = torch.zeros_like(src)
+    d.propagators_dev(src, x, rtol=RTOL, maxiter=MAXITER, solver=T.SOLVER_EO_MIXED)  # warm-up
+    A.check(A.lib().dwf_eo_phase_profile(d.handle, 1), d.handle)
+    infos = d.propagators_dev(src, x, rtol=RTOL, maxiter=MAXITER, solver=T.SOLVER_EO_MIXED)
+    ms = (C.c_double * 8)()
+    cnt = (C.c_uint64 * 8)()
+    A.check(A.lib().dwf_eo_phase_times(d.handle, ms, cnt), d.handle)
+    names = ["hop_M5inv", "M5_minus_hop", "alpha_reduction", "adjoint_hop_M5inv",
+             "adjoint_combine_update", "beta_reduction_reliable_updates", "direction_update"]
+    out = {n: {"ms": round(ms[k], 3), "count": int(cnt[k]),
+               "us_per_iteration": round(1e3 * ms[k] / max(1, cnt[k]), 2)} for k, n in enumerate(names)}
+    print(json.dumps({"eo_phases": out, "schur_iterations_mean": statistics.mean(
+        i["schur_iterations"] for i in infos)}))
+    d.close()
+    return 0
+
+
 def dslash_variants():
     """Event-timed GB/s of both Dslash kernels (site, column) in FP64 and FP32
     at 256x256x16 and 512x512x16 (one JSON line)."""
@@ -807,6 +834,7 @@ def main():
     ap.add_argument("--profile-dslash", action="store_true")
     ap.add_argument("--profile-learned", action="store_true")
     ap.add_argument("--dslash-variants", action="store_true")
+    ap.add_argument("--eo-phases", action="store_true")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
@@ -816,6 +844,8 @@ def main():
         return profile_learned()
     if args.dslash_variants:
         return dslash_variants()
+    if args.eo_phases:
+        return eo_phases()
     if args.calibrate_reference:
         return calibrate_reference()
     if args.warmup < 3 and args.impl == "ours":

@@ -347,6 +347,15 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
 int dwf_set_dslash_variant(dwf_ctx* ctx, int variant);
 int dwf_dslash_variant(const dwf_ctx* ctx, int precision, int nrhs);
 
+/* Per-phase device timers of the even-odd solver kernel (block 0's view, each
+ * phase including the grid barrier that ends it): enable (1) allocates and
+ * zeroes them, 0 frees them (off by default: no cost). dwf_eo_phase_times
+ * returns accumulated ms and counts for the phases 0 hop + M5^-1, 1 M5 - H
+ * (|t|^2), 2 alpha reduction, 3 adjoint hop + M5^-1, 4 adjoint combine and
+ * x, r update, 5 beta reduction and reliable updates, 6 direction update. */
+int dwf_eo_phase_profile(dwf_ctx* ctx, int enable);
+int dwf_eo_phase_times(dwf_ctx* ctx, double* ms, uint64_t* counts);
+
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);
 /* Accumulated device time (ms) of the persistent solver launches of one kind

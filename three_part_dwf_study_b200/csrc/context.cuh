@@ -80,6 +80,7 @@ struct dwf_ctx
     float2* eo_t32 = nullptr;
     float2* eo_y32 = nullptr;
     float2* eo_e32 = nullptr;
+    unsigned long long* eo_phase = nullptr;  // per-phase timers (dwf_eo_phase_profile)
 
     // HMC workspace (allocated on first use)
     double* h_mom = nullptr;    // [2V]

@@ -25,6 +25,21 @@ namespace {
 
 constexpr int kEven = 0, kOdd = 1;
 
+// Phase timer (block 0, thread 0; only when a phase buffer is given): adds the
+// time since the previous mark to slot k. Phases: 0 P1, 1 P2, 2 the alpha
+// reduction, 3 P3, 4 P4, 5 the beta reduction and reliable updates, 6 P5, each
+// including the grid barrier that ends it.
+__device__ __forceinline__ void phase_mark(unsigned long long* ph, int k, unsigned long long& t)
+{
+    if (ph && blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        const unsigned long long n = globaltimer_ns();
+        ph[k] += n - t;
+        ph[8 + k] += 1;
+        t = n;
+    }
+}
+
 template <typename R>
 struct NoLd
 {
@@ -173,6 +188,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
     Spinor<float>* zs = reinterpret_cast<Spinor<float>*>(
         reinterpret_cast<char*>(sm_all) + ((solver_smem_bytes(d.nrhs) + 15) & ~size_t(15))) + threadIdx.x;
 
+    unsigned long long ph_t = globaltimer_ns();
     for (int it = 1; it <= d.maxiter && nact > 0; ++it)
     {
         // P1: y = M5^-1 H_eo p
@@ -191,6 +207,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                     });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
+        phase_mark(e.phase_ns, 0, ph_t);
         // P2: t = M5 p - H_oe y, |t|^2
         sweep_sites(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, true,
                     [&](int j, int i, long uo) {
@@ -204,6 +221,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                     });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
+        phase_mark(e.phase_ns, 1, ph_t);
         reduce_listed(d, s.act, nact, 0, s.aux);
         for (int k = threadIdx.x; k < nact; k += blockDim.x)
         {
@@ -218,6 +236,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
         }
         __syncthreads();
         nact = compact(d.nrhs, s.act, s.scratch, [&](int j) { return s.state[j] == RHS_ACTIVE; });
+        phase_mark(e.phase_ns, 2, ph_t);
         // P3: y = M5^dag^-1 H^dag_eo t
         sweep_sites(d, s.act, nact, nsite4, e.nch4, e.ch4, s.scratch, false,
                     [&](int j, int h, long uo) {
@@ -234,6 +253,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                     });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
+        phase_mark(e.phase_ns, 3, ph_t);
         // P4: Ap = M5^dag t - H^dag_oe y; e += alpha p; r -= alpha Ap
         sweep_sites(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, true,
                     [&](int j, int i, long uo) {
@@ -253,6 +273,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                     });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
+        phase_mark(e.phase_ns, 4, ph_t);
         reduce_listed(d, s.act, nact, 0, s.aux);
         for (int k = threadIdx.x; k < nact; k += blockDim.x)
         {
@@ -349,6 +370,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
         nact = compact(d.nrhs, s.act, s.scratch, [&](int j) { return s.state[j] == RHS_ACTIVE; });
         if (nact == 0)
             break;
+        phase_mark(e.phase_ns, 5, ph_t);
         // P5: p = r + beta p
         sweep_sites(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, false,
                     [&](int j, int i, long uo) {
@@ -359,6 +381,7 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                     });
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
+        phase_mark(e.phase_ns, 6, ph_t);
     }
     write_outputs(d, s);
 }

@@ -42,6 +42,7 @@ struct EoDesc
     float2* y32;
     double2* xn64;  // reliable update: x + e parked here
     int zsmem;      // 1: the FP32 hop + M5^-1 phases keep the slices in shared memory
+    unsigned long long* phase_ns;  // optional [16]: per-phase ns [0, 8) and counts [8, 16)
 };
 
 // Hop term H (DAG = false) or H^dag of the site (s, t, x), reading the other

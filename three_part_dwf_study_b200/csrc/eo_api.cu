@@ -139,6 +139,7 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
         e.y64 = c->eo_y;
         e.y32 = c->eo_y32;
         e.xn64 = c->eo_xn;
+        e.phase_ns = c->eo_phase;
 
         const void* fn = reinterpret_cast<const void*>(&cg_eo_mixed_kernel);
         // the FP32 hop + M5^-1 phases keep each thread's Ls slices in shared
@@ -205,3 +206,41 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
 }
 
 }  // namespace dwfb
+
+extern "C" {
+
+int dwf_eo_phase_profile(dwf_ctx* c, int enable)
+{
+    if (!c)
+        return DWF_BAD_ARG;
+    CK(cudaSetDevice(c->device));
+    if (enable && !c->eo_phase)
+        CK(cudaMalloc(&c->eo_phase, 16 * sizeof(unsigned long long)));
+    if (!enable && c->eo_phase)
+    {
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFree(c->eo_phase);
+        c->eo_phase = nullptr;
+    }
+    if (c->eo_phase)
+        CK(cudaMemsetAsync(c->eo_phase, 0, 16 * sizeof(unsigned long long), c->stream));
+    return DWF_OK;
+}
+
+int dwf_eo_phase_times(dwf_ctx* c, double* ms, uint64_t* counts)
+{
+    if (!c || !c->eo_phase || !ms)
+        return DWF_BAD_ARG;
+    unsigned long long h[16];
+    CK(cudaMemcpyAsync(h, c->eo_phase, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 8; ++k)
+    {
+        ms[k] = double(h[k]) * 1e-6;
+        if (counts)
+            counts[k] = h[8 + k];
+    }
+    return DWF_OK;
+}
+
+}  // extern "C"

@@ -801,7 +801,7 @@ def dslash_variants():
         for prec, dt, w in ((64, torch.float64, 8), (32, torch.float32, 4)):
             a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
             b = torch.empty_like(a)
-            for v, name in ((0, "site"), (1, "column")):
+            for v, name in ((0, "site"), (1, "column"), (2, "site_shuffle")):
                 A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
                 for _ in range(3):
                     d.apply_dev(0, a, b)

@@ -340,9 +340,11 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
 
 /* Dslash kernel variant for dwf_apply[_dev]: 0 = one thread per 5-D site,
  * 1 = one thread per 4-D site sweeping the fifth dimension (links and fifth-
- * dimension neighbours kept in registers), -1 = autotune (default): the first
- * application per (precision, batch-size bucket) times both with CUDA events
- * and keeps the faster. dwf_dslash_variant reports the choice in force for a
+ * dimension neighbours kept in registers), 2 = one thread per 5-D site with
+ * the x neighbours exchanged by warp shuffles (Nx a multiple of 32; else as
+ * 0), -1 = autotune (default): the first application per (precision,
+ * batch-size bucket) times the variants with CUDA events and keeps the
+ * fastest. dwf_dslash_variant reports the choice in force for a
  * precision and batch size (-1 if not tuned yet). */
 int dwf_set_dslash_variant(dwf_ctx* ctx, int variant);
 int dwf_dslash_variant(const dwf_ctx* ctx, int precision, int nrhs);

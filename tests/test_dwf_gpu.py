@@ -199,11 +199,14 @@ def test_bounded_barrier_times_out_and_context_survives(tdwf):
     assert r.converged and r.info["true_relres"] < 1e-9
 
 
-@pytest.mark.parametrize("variant", [0, 1])
-@pytest.mark.parametrize("shape", [(8, 8, 4), (13, 37, 3), (64, 64, 16), (5, 3, 1), (16, 40, 24)])
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(8, 8, 4), (13, 37, 3), (64, 64, 16), (5, 3, 1), (16, 40, 24),
+                                   (6, 32, 2), (3, 96, 5)])
 def test_dslash_variants_match_oracle(tdwf, variant, shape):
-    """Both Dslash kernels (one thread per 5-D site; one thread per 4-D site
-    sweeping the fifth dimension) in FP64 and FP32, ragged tile edges included."""
+    """The Dslash kernels (one thread per 5-D site; one thread per 4-D site
+    sweeping the fifth dimension; one thread per 5-D site with warp-shuffled x
+    neighbours, which takes Nx % 32 == 0 and otherwise runs as the first) in
+    FP64 and FP32, ragged tile edges and row/warp boundaries included."""
     torch = pytest.importorskip("torch")
     from three_part_dwf_study_b200 import _capi as A
     Nt, Nx, Ls = shape

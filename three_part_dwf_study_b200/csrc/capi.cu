@@ -137,7 +137,14 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
                            ? std::min(nb, std::max(1, DWFB_DIRAC_BLOCKS_PER_SM * c->nsm))
                            : nb;
         const dim3 grid(bx, nrhs);
-        if (dag)
+        if (variant == 2 && c->L.Nx % 32 == 0)
+        {
+            if (dag)
+                dirac_warp_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+            else
+                dirac_warp_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        }
+        else if (dag)
             dirac_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
         else
             dirac_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
@@ -145,8 +152,10 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
     c->launches += 1;
 }
 
-// Autotuner: time both variants (two applications each, CUDA events on the
-// context stream) for this precision and batch-size bucket, keep the faster.
+// Autotuner: time the variants (two applications each, CUDA events on the
+// context stream) for this precision and batch-size bucket, keep the fastest:
+// 0 one thread per 5-D site, 1 one thread per 4-D column, 2 one thread per 5-D
+// site with warp-shuffled x neighbours (Nx a multiple of 32).
 template <typename R>
 int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<R>* in,
                  cplx<R>* out, const cplx<R>* U)
@@ -162,7 +171,8 @@ int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<
         return it->second;
     float best = 1e30f;
     int choice = 0;
-    for (int v = 0; v < 2; ++v)
+    const int nvar = (c->L.Nx % 32 == 0) ? 3 : 2;
+    for (int v = 0; v < nvar; ++v)
     {
         launch_dirac<R>(c, v, false, nrhs, conf_d, conf0, in, out, U);  // warm-up
         cudaEventRecord(c->ev0, c->stream);
@@ -823,7 +833,7 @@ uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
 
 int dwf_set_dslash_variant(dwf_ctx* c, int variant)
 {
-    if (!c || variant < -1 || variant > 1)
+    if (!c || variant < -1 || variant > 2)
         return DWF_BAD_ARG;
     c->dslash_variant = variant;
     if (variant == -1)

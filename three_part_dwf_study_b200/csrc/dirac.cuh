@@ -136,6 +136,98 @@ __device__ __forceinline__ Spinor<R> dirac_site(const cplx<R>* __restrict__ in,
     return dirac_site_ld<DAG, R>(FieldLd<R>{in}, U, L, s, t, x);
 }
 
+// Shuffle of a complex number / spinor between lanes of a full warp.
+__device__ __forceinline__ double2 shfl_c(double2 v, int src)
+{
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+__device__ __forceinline__ float2 shfl_c(float2 v, int src)
+{
+    return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// The operator at (s, t, x) for a warp whose 32 lanes hold x = x0 .. x0 + 31 of
+// one row (Nx a multiple of 32): the x +- 1 neighbours and the backward x link
+// come from the adjacent lanes by shuffle (lanes 0 and 31 load theirs), so a
+// site issues 3 spinor loads for the 4-D hop instead of 5.
+template <bool DAG, typename R>
+__device__ __forceinline__ Spinor<R> dirac_site_warp(const cplx<R>* __restrict__ in,
+                                                     const cplx<R>* __restrict__ U, const Lat& L,
+                                                     int s, int t, int x, int lane)
+{
+    using T = cplx<R>;
+    const int Nt = L.Nt, Nx = L.Nx;
+    const int tp = (t + 1 == Nt) ? 0 : t + 1;
+    const int tm = (t == 0) ? Nt - 1 : t - 1;
+    const int xp = (x + 1 == Nx) ? 0 : x + 1;
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+    const long sb = long(s) * L.V;
+    const int here = t * Nx + x;
+
+    const Spinor<R> c = ld_spinor(in, sb + here);
+    const T Ux = U[L.V + here];
+    // neighbours in x from the adjacent lanes (same row, consecutive x)
+    const int up = (lane == 31) ? 31 : lane + 1, dn = (lane == 0) ? 0 : lane - 1;
+    Spinor<R> vxp{shfl_c(c.s0, up), shfl_c(c.s1, up)};
+    Spinor<R> vxm{shfl_c(c.s0, dn), shfl_c(c.s1, dn)};
+    T Uxm = shfl_c(Ux, dn);
+    if (lane == 31)
+        vxp = ld_spinor(in, sb + t * Nx + xp);
+    if (lane == 0)
+    {
+        vxm = ld_spinor(in, sb + t * Nx + xm);
+        Uxm = U[L.V + t * Nx + xm];
+    }
+    const Spinor<R> vtp = ld_spinor(in, sb + tp * Nx + x);
+    const Spinor<R> vtm = ld_spinor(in, sb + tm * Nx + x);
+    const T Ut = U[here];
+    const T Utm = U[tm * Nx + x];
+
+    const R stp = (t == Nt - 1) ? R(L.bct) : R(1);
+    const R stm = (t == 0) ? R(L.bct) : R(1);
+    const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
+    const R sxm = (x == 0) ? R(L.bcx) : R(1);
+    constexpr R kf = DAG ? R(1) : R(-1);
+    constexpr R kb = -kf;
+
+    T w = cmul(Ut, stp * (vtp.s0 + kf * vtp.s1));
+    T upv = w;
+    T lo = kf * w;
+    w = cmulc(Utm, stm * (vtm.s0 + kb * vtm.s1));
+    upv += w;
+    lo += kb * w;
+    w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
+    upv += w;
+    lo += kf * itimes(w);
+    w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
+    upv += w;
+    lo += kb * itimes(w);
+
+    const R dg = R(L.diag);
+    Spinor<R> o;
+    o.s0 = dg * c.s0 - R(0.5) * upv;
+    o.s1 = dg * c.s1 - R(0.5) * lo;
+    if (L.fifth)
+    {
+        const int Ls = L.Ls;
+        const int sup = (s + 1 == Ls) ? 0 : s + 1;
+        const R cup = (s + 1 == Ls) ? R(L.mf) : R(-1);
+        const int sdn = (s == 0) ? Ls - 1 : s - 1;
+        const R cdn = (s == 0) ? R(L.mf) : R(-1);
+        if (!DAG)
+        {
+            o.s1 += cup * in[2 * (long(sup) * L.V + here) + 1];
+            o.s0 += cdn * in[2 * (long(sdn) * L.V + here)];
+        }
+        else
+        {
+            o.s1 += cdn * in[2 * (long(sdn) * L.V + here) + 1];
+            o.s0 += cup * in[2 * (long(sup) * L.V + here)];
+        }
+    }
+    return o;
+}
+
 // Site index i in [0, Ls*V) -> (s, t, x), x fastest (the reference layout).
 __device__ __forceinline__ void site_coords(const Lat& L, int i, int& s, int& t, int& x)
 {

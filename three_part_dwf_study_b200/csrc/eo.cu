@@ -149,7 +149,7 @@ template __global__ void eo_combine_kernel<true>(Lat, EoGeo, const double2*, con
 // ---- persistent mixed-precision Schur CG ------------------------------------
 
 #ifndef DWFB_EO_MINB
-#define DWFB_EO_MINB 3  // resident 256-thread blocks per SM the register budget targets
+#define DWFB_EO_MINB 2  // resident 256-thread blocks per SM the register budget targets (2: no spills)
 #endif
 
 __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e)

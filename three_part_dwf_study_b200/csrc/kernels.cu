@@ -36,6 +36,40 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// One thread per 5-D site, warps over 32 consecutive x of one row (Nx a
+// multiple of 32), x neighbours by shuffle; the loop is warp-uniform.
+template <bool DAG, typename R>
+__global__ void __launch_bounds__(256)
+    dirac_warp_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out, long fsz,
+                      const cplx<R>* __restrict__ U, long usz, const int* __restrict__ conf,
+                      int conf0)
+{
+    const int j = blockIdx.y;
+    const int c = conf ? conf[j] : conf0;
+    const cplx<R>* Uj = U + long(c) * usz;
+    const cplx<R>* inj = in + j * fsz;
+    cplx<R>* outj = out + j * fsz;
+    const int lane = threadIdx.x & 31;
+    // L.nsite is a multiple of 32 (Nx is), so every warp's 32 sites are valid
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < L.nsite;
+         base += gridDim.x * blockDim.x)
+    {
+        const int i = base + lane;
+        int s, t, x;
+        site_coords(L, i, s, t, x);
+        st_spinor(outj, i, dirac_site_warp<DAG, R>(inj, Uj, L, s, t, x, lane));
+    }
+}
+
+template __global__ void dirac_warp_kernel<false, double>(Lat, const double2*, double2*, long,
+                                                          const double2*, long, const int*, int);
+template __global__ void dirac_warp_kernel<true, double>(Lat, const double2*, double2*, long,
+                                                         const double2*, long, const int*, int);
+template __global__ void dirac_warp_kernel<false, float>(Lat, const float2*, float2*, long,
+                                                         const float2*, long, const int*, int);
+template __global__ void dirac_warp_kernel<true, float>(Lat, const float2*, float2*, long,
+                                                        const float2*, long, const int*, int);
+
 // One thread per 4-D site, all Ls slices (links and the fifth-dimension
 // neighbours reused from registers); blocks are 32 x 8 tiles of (x, t) so the
 // t +- 1 neighbours of a warp are mostly loaded by the block's other warps.

@@ -15,6 +15,13 @@ __global__ void dirac_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __r
                              long fsz, const cplx<R>* __restrict__ U, long usz,
                              const int* __restrict__ conf, int conf0);
 
+// Same operator, one thread per 5-D site with the x neighbours exchanged by
+// warp shuffles (needs Nx % 32 == 0).
+template <bool DAG, typename R>
+__global__ void dirac_warp_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                                  long fsz, const cplx<R>* __restrict__ U, long usz,
+                                  const int* __restrict__ conf, int conf0);
+
 // Same operator, one thread per 4-D site sweeping the fifth dimension
 // (grid: ceil(Nx/32) x ceil(Nt/8) x nrhs, 256 threads).
 template <bool DAG, typename R>

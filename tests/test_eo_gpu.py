@@ -76,3 +76,25 @@ def test_eo_falls_back_on_odd_lattices(T):
     x, info = d.propagators(src, rtol=1e-10, maxiter=5000, solver=T.SOLVER_EO_MIXED)
     assert all(i["converged"] and i["true_relres"] <= 1e-10 and i["schur_iterations"] == 0
                for i in info)
+
+
+def test_eo_phase_timers(T):
+    """The even-odd kernel's optional phase timers count one entry per Schur
+    iteration for each operator phase, and cost nothing when off."""
+    import ctypes as C
+    from three_part_dwf_study_b200 import _capi as A
+    rng = np.random.default_rng(3)
+    d = T.DomainWall(16, 12, 8, 1.0, 0.1)
+    d.set_gauge(random_theta(rng, 16, 12))
+    src = boundary_sources(rng, 16, 12, 8, 2)
+    ms = (C.c_double * 8)()
+    cnt = (C.c_uint64 * 8)()
+    assert A.lib().dwf_eo_phase_times(d.handle, ms, cnt) == A.DWF_BAD_ARG  # off by default
+    assert A.lib().dwf_eo_phase_profile(d.handle, 1) == 0
+    _, info = d.propagators(src, rtol=1e-10, maxiter=20000, solver=T.SOLVER_EO_MIXED)
+    assert A.lib().dwf_eo_phase_times(d.handle, ms, cnt) == 0
+    it = max(i["schur_iterations"] for i in info)
+    assert cnt[0] == cnt[1] == cnt[3] == cnt[4] == it
+    assert all(ms[k] > 0.0 for k in (0, 1, 3, 4))
+    assert A.lib().dwf_eo_phase_profile(d.handle, 0) == 0
+    d.close()

@@ -386,6 +386,56 @@ def hmc_compare(T, d, rank, ntraj):
     return res
 
 
+def wilson_learned_grid(T, ntrain=8):
+    """Wilson 64x64 near the critical mass: the learned preconditioner (4
+    layers, 8 hidden complex channels) trained on ntrain seeded configurations
+    per (beta, m0), then 16 point-source propagator solves to 1e-10 on a
+    held-out configuration, against the plain FP64 CG (CGNR) and the mixed CG
+    on the same GPU. Device time per batch (CUDA events on the library
+    stream, host copies of sources and solutions included), iterations and
+    operator applications."""
+    import torch
+    from three_part_dwf_study_b200.ensemble import quenched_ensemble
+    L = 64
+    out = {"lattice": [L, L], "hidden": 8, "sources": 16, "rtol": RTOL, "settings": {}}
+    for beta in (2.0, 3.0, 4.0, 6.0):
+        for m0 in (-0.05, 0.05):
+            w = T.Wilson(L, L, m0, beta)
+            st = torch.cuda.ExternalStream(w.stream_ptr())
+            w.set_gauge(quenched_ensemble(GAUGE_SEED + int(10 * beta), ntrain, L, L, beta))
+            w.lp_init(hidden=8, seed=1)
+            tinfo = w.lp_train(steps=3000, batch=8, lr=3e-3, lr_decay_steps=1000, pairs_per_conf=32,
+                               solver_iters=50, solver_every=2, seed=3)
+            w.set_gauge(quenched_ensemble(GAUGE_SEED + 7 + int(10 * beta), 1, L, L, beta))
+            src = np.zeros((16, w.Ndof), np.complex128)
+            for k in range(16):
+                src[k, ((4 * k) * L) * 2 + (k % 2)] = 1.0
+            row = {"training_loss": tinfo["loss_last"]}
+            for name, sv in (("learned", T.SOLVER_LEARNED), ("plain_fp64_cg", T.SOLVER_CG64),
+                             ("mixed_cg", T.SOLVER_MIXED)):
+                w.propagators(src, rtol=RTOL, maxiter=50000, solver=sv)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(st)
+                _, infos = w.propagators(src, rtol=RTOL, maxiter=50000, solver=sv)
+                e1.record(st)
+                e1.synchronize()
+                if not all(i["converged"] for i in infos):
+                    raise SystemExit(f"Wilson solve did not converge: {name} beta={beta} m={m0}")
+                it = statistics.mean(i["schur_iterations"] if sv == T.SOLVER_LEARNED else i["iterations"]
+                                     for i in infos)
+                row[name] = {"ms_per_batch": e0.elapsed_time(e1), "iterations_mean": it,
+                             "operator_applications_mean": 2 * it}
+            row["operator_application_ratio_plain_over_learned"] = \
+                row["plain_fp64_cg"]["operator_applications_mean"] / row["learned"]["operator_applications_mean"]
+            row["time_ratio_plain_over_learned"] = \
+                row["plain_fp64_cg"]["ms_per_batch"] / row["learned"]["ms_per_batch"]
+            out["settings"][f"beta={beta},m={m0}"] = row
+            w.close()
+    return out
+
+
 def workload_config(solver):
     return {
         "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, seeded beta=3.0 "
@@ -580,6 +630,8 @@ def impl_ours(args):
 
     # ---- HMC on the same lattice: FP64 and mixed CG on the same trajectories ----
     hmc = hmc_compare(T, d, rank, args.hmc_trajectories)
+    # ---- Wilson 64x64 near the critical mass with the learned preconditioner ----
+    wil = wilson_learned_grid(T) if (args.wilson_learned and ws == 1) else None
 
     # ---- roofline of the dominant kernel (the persistent even-odd solver) ----
     V = NT * NX
@@ -660,6 +712,7 @@ def impl_ours(args):
         "roofline": roofline,
         "dslash": dslash,
         "hmc": hmc,
+        "learned_wilson_64x64": wil,
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -739,8 +792,9 @@ def profile_learned():
 
 
 def profile_dslash():
-    """Two applications of D at the Dslash bench lattice for each kernel
-    variant and precision (for ncu)."""
+    """One application of D at the Dslash bench lattice for each kernel
+    variant (site, column, site with shuffled x neighbours, t sweep) in FP64,
+    then in FP32 (for ncu)."""
     import torch
     import three_part_dwf_study_b200 as T
     from three_part_dwf_study_b200 import _capi as A
@@ -750,10 +804,9 @@ def profile_dslash():
     for dt in (torch.float64, torch.float32):
         a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
         b = torch.empty_like(a)
-        for v in (0, 1):
+        for v in (0, 1, 2, 3):
             A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
-            for _ in range(2):
-                d.apply_dev(0, a, b)
+            d.apply_dev(0, a, b)
     d.sync()
     d.close()
     return 0
@@ -787,8 +840,9 @@ def eo_phases():
 
 
 def dslash_variants():
-    """Event-timed GB/s of both Dslash kernels (site, column) in FP64 and FP32
-    at 256x256x16 and 512x512x16 (one JSON line)."""
+    """Event-timed GB/s of the Dslash kernels (site, column, site with shuffled
+    x neighbours, t sweep at the automatic and at fixed chunk lengths) in FP64
+    and FP32 at 256x256x16 and 512x512x16 (one JSON line)."""
     import torch
     import three_part_dwf_study_b200 as T
     from three_part_dwf_study_b200 import _capi as A
@@ -801,7 +855,11 @@ def dslash_variants():
         for prec, dt, w in ((64, torch.float64, 8), (32, torch.float32, 4)):
             a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
             b = torch.empty_like(a)
-            for v, name in ((0, "site"), (1, "column"), (2, "site_shuffle")):
+            for v, chunk, name in ((0, 0, "site"), (1, 0, "column"), (2, 0, "site_shuffle"),
+                                   (3, 0, "t_sweep_auto"), (3, 8, "t_sweep_8"),
+                                   (3, 16, "t_sweep_16"), (3, 32, "t_sweep_32"),
+                                   (3, 64, "t_sweep_64")):
+                A.check(A.lib().dwf_set_dslash_chunk(d.handle, chunk), d.handle)
                 A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
                 for _ in range(3):
                     d.apply_dev(0, a, b)
@@ -830,6 +888,8 @@ def main():
     ap.add_argument("--calibrate-reference", action="store_true")
     ap.add_argument("--hmc-trajectories", type=int, default=2,
                     help="HMC trajectories compared between FP64 and mixed CG (0: skip)")
+    ap.add_argument("--no-wilson-learned", dest="wilson_learned", action="store_false",
+                    help="skip the Wilson 64x64 learned-preconditioner grid")
     ap.add_argument("--profile-case", action="store_true")
     ap.add_argument("--profile-dslash", action="store_true")
     ap.add_argument("--profile-learned", action="store_true")

@@ -342,12 +342,19 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
  * 1 = one thread per 4-D site sweeping the fifth dimension (links and fifth-
  * dimension neighbours kept in registers), 2 = one thread per 5-D site with
  * the x neighbours exchanged by warp shuffles (Nx a multiple of 32; else as
- * 0), -1 = autotune (default): the first application per (precision,
- * batch-size bucket) times the variants with CUDA events and keeps the
- * fastest. dwf_dslash_variant reports the choice in force for a
+ * 0), 3 = one thread per (s, x) sweeping a chunk of rows in t, the rows
+ * streamed through a shared-memory ring by cp.async (Nx a multiple of 32 and
+ * Ls <= 16; else as 0), -1 = autotune (default): the first application per
+ * (precision, batch-size bucket) times the variants with CUDA events and
+ * keeps the fastest. dwf_dslash_variant reports the choice in force for a
  * precision and batch size (-1 if not tuned yet). */
 int dwf_set_dslash_variant(dwf_ctx* ctx, int variant);
 int dwf_dslash_variant(const dwf_ctx* ctx, int precision, int nrhs);
+
+/* Rows per chunk of variant 3 (0 = automatic: halved from Nt, down to 8,
+ * until the grid holds two blocks per resident slot). Clears the autotuner's
+ * choices. */
+int dwf_set_dslash_chunk(dwf_ctx* ctx, int rows);
 
 /* Per-phase device timers of the even-odd solver kernel (block 0's view, each
  * phase including the grid barrier that ends it): enable (1) allocates and

@@ -199,14 +199,17 @@ def test_bounded_barrier_times_out_and_context_survives(tdwf):
     assert r.converged and r.info["true_relres"] < 1e-9
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 @pytest.mark.parametrize("shape", [(8, 8, 4), (13, 37, 3), (64, 64, 16), (5, 3, 1), (16, 40, 24),
-                                   (6, 32, 2), (3, 96, 5)])
+                                   (6, 32, 2), (3, 96, 5), (9, 128, 4), (20, 64, 1)])
 def test_dslash_variants_match_oracle(tdwf, variant, shape):
     """The Dslash kernels (one thread per 5-D site; one thread per 4-D site
     sweeping the fifth dimension; one thread per 5-D site with warp-shuffled x
-    neighbours, which takes Nx % 32 == 0 and otherwise runs as the first) in
-    FP64 and FP32, ragged tile edges and row/warp boundaries included."""
+    neighbours, which takes Nx % 32 == 0 and otherwise runs as the first; one
+    thread per (s, x) sweeping a chunk of rows in t, which takes Nx % 32 == 0
+    and Ls <= 16 and otherwise runs as the first) in FP64 and FP32, ragged
+    tile edges, row/warp boundaries, several x tiles per block (9x128x4,
+    20x64x1) and ragged t chunks included."""
     torch = pytest.importorskip("torch")
     from three_part_dwf_study_b200 import _capi as A
     Nt, Nx, Ls = shape
@@ -224,3 +227,47 @@ def test_dslash_variants_match_oracle(tdwf, variant, shape):
         d.apply_dev(op, x32, y32)
         assert rel(y32.cpu().numpy(), ref) < 2e-6, name
     assert A.lib().dwf_dslash_variant(d.handle, 64, 2) == variant
+
+
+@pytest.mark.parametrize("chunk", [1, 2, 3, 7, 13, 40])
+@pytest.mark.parametrize("shape", [(13, 64, 6), (40, 32, 16)])
+def test_dslash_sweep_chunks(tdwf, chunk, shape):
+    """The t-sweeping Dslash at fixed chunk lengths: one-row chunks, chunks
+    that do not divide Nt, and one chunk longer than Nt; three fields."""
+    torch = pytest.importorskip("torch")
+    from three_part_dwf_study_b200 import _capi as A
+    Nt, Nx, Ls = shape
+    rng = np.random.default_rng(chunk * 31 + Nt)
+    d = tdwf.DomainWall(Nt, Nx, Ls, 1.7, 0.05)
+    o = O.Dwf(Nt, Nx, Ls, 1.7, 0.05)
+    assert A.lib().dwf_set_dslash_variant(d.handle, 3) == 0
+    assert A.lib().dwf_set_dslash_chunk(d.handle, chunk) == 0
+    th = random_theta(rng, Nt, Nx)
+    psi = random_field(rng, 3 * o.ndof)
+    for op, name in OPS:
+        ref = np.concatenate([o.apply(op, th, psi[k * o.ndof:(k + 1) * o.ndof]) for k in range(3)])
+        assert rel(d.apply(op, th, psi), ref) < 1e-13, name
+        x32 = torch.from_numpy(psi.astype(np.complex64)).cuda()
+        y32 = torch.empty_like(x32)
+        d.apply_dev(op, x32, y32)
+        assert rel(y32.cpu().numpy(), ref) < 2e-6, name
+    assert A.lib().dwf_set_dslash_chunk(d.handle, -1) != 0
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("shape", [(16, 256), (7, 96), (12, 64)])
+def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
+    """The Wilson operator (no fifth dimension, antiperiodic in both
+    directions) through every Dslash kernel; 16x256 puts eight 32-x tiles in
+    one block of the t-sweeping kernel."""
+    from three_part_dwf_study_b200 import _capi as A
+    Nt, Nx = shape
+    rng = np.random.default_rng(Nt + Nx)
+    w = tdwf.Wilson(Nt, Nx, -0.3, 0.0, bc_t=-1.0, bc_x=-1.0)
+    o = O.Wilson(Nt, Nx, -0.3, -1.0, -1.0)
+    assert A.lib().dwf_set_dslash_variant(w.handle, variant) == 0
+    th = random_theta(rng, Nt, Nx)
+    psi = random_field(rng, 2 * o.ntot)
+    for op, name in OPS:
+        ref = np.concatenate([o.apply(op, th, psi[:o.ntot]), o.apply(op, th, psi[o.ntot:])])
+        assert rel(w.apply(op, th, psi), ref) < 1e-13, name

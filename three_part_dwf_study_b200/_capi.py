@@ -102,6 +102,7 @@ SIGNATURES = {
     "dwf_launch_count": (C.c_uint64, [_P]),
     "dwf_set_dslash_variant": (_I, [_P, _I]),
     "dwf_dslash_variant": (_I, [_P, _I, _I]),
+    "dwf_set_dslash_chunk": (_I, [_P, _I]),
     "dwf_barrier_selftest": (_I, [_P, _I, C.c_uint64]),
     "dwf_cg_noalloc": (_I, [C.POINTER(DwfParams), _I, _P, _P, _P, _I, _D, _I, _P,
                             C.POINTER(SolveInfo)]),

@@ -117,12 +117,66 @@ int ensure_part(dwf_ctx* c, size_t n)
 namespace {
 
 // One application of D (dag = false) or D^dag with the chosen kernel variant.
+// The t-sweeping kernel needs whole 32-lane rows and a block of all Ls slices.
+bool sweep_ok(const Lat& L) { return L.Nx % 32 == 0 && 32 * L.Ls <= 512; }
+
+struct SweepShape
+{
+    int g;   // 32-x tiles per block
+    int tc;  // rows per chunk
+};
+
+// Blocks of up to 512 threads (G tiles of 32 x 32 Ls threads); the chunk
+// length is the context's setting, else halved from Nt (down to 8 rows) until
+// the grid holds at least two blocks per resident slot (1024 resident threads
+// per SM, as the kernel's launch bounds allow), so the tail of the launch
+// stays short.
+SweepShape sweep_shape(const dwf_ctx* c, int nrhs, int resident_threads)
+{
+    const Lat& L = c->L;
+    int g = 1;
+    while (32 * L.Ls * g * 2 <= 512 && (L.Nx / 32) % (g * 2) == 0)
+        g *= 2;
+    const long nxt = L.Nx / (32 * g);
+    int tc = c->dslash_chunk > 0 ? std::min(c->dslash_chunk, L.Nt) : L.Nt;
+    if (c->dslash_chunk <= 0)
+    {
+        const long slots = long(c->nsm) * std::max(1, resident_threads / (32 * L.Ls * g));
+        while (tc > 8 && nxt * ((L.Nt + tc - 1) / tc) * nrhs < 2 * slots)
+            tc = (tc + 1) / 2;
+    }
+    return {g, tc};
+}
+
 template <typename R>
 void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d, int conf0,
                   const cplx<R>* in, cplx<R>* out, const cplx<R>* U)
 {
     const long fs = c->fsz();
-    if (variant == 1)
+    if (variant == 3 && sweep_ok(c->L))
+    {
+        constexpr int S = sizeof(R) == 8 ? kSweepSlots64 : kSweepSlots32;
+        const SweepShape sh = sweep_shape(c, nrhs, 1024);
+        const dim3 grid(c->L.Nx / (32 * sh.g), (c->L.Nt + sh.tc - 1) / sh.tc, nrhs);
+        const dim3 block(32, c->L.Ls, sh.g);
+        const size_t smem = S * sweep_slot_bytes(c->L.Ls, sh.g, sizeof(cplx<R>));
+        auto kern = dag ? dirac_sweep_kernel<true, R, S> : dirac_sweep_kernel<false, R, S>;
+        const int bit = (dag ? 1 : 0) + (sizeof(R) == 8 ? 2 : 0);
+        if (!(c->sweep_smem_set & (1 << bit)))
+        {
+            // the largest ring this context's lattice can ask for (G = 1 .. 512 / (32 Ls));
+            // a failure here leaves the launch below to fail, which the caller's
+            // cudaGetLastError check reports
+            size_t most = 0;
+            for (int g = 1; 32 * c->L.Ls * g <= 512; g *= 2)
+                most = std::max(most, S * sweep_slot_bytes(c->L.Ls, g, sizeof(cplx<R>)));
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most)) ==
+                cudaSuccess)
+                c->sweep_smem_set |= 1 << bit;
+        }
+        kern<<<grid, block, smem, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0, sh.tc);
+    }
+    else if (variant == 1)
     {
         const dim3 grid((c->L.Nx + 31) / 32, (c->L.Nt + 7) / 8, nrhs);
         if (dag)
@@ -155,7 +209,8 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
 // Autotuner: time the variants (two applications each, CUDA events on the
 // context stream) for this precision and batch-size bucket, keep the fastest:
 // 0 one thread per 5-D site, 1 one thread per 4-D column, 2 one thread per 5-D
-// site with warp-shuffled x neighbours (Nx a multiple of 32).
+// site with warp-shuffled x neighbours (Nx a multiple of 32), 3 one thread per
+// (s, x) sweeping a chunk of rows in t (Nx a multiple of 32, Ls <= 16).
 template <typename R>
 int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<R>* in,
                  cplx<R>* out, const cplx<R>* U)
@@ -171,9 +226,10 @@ int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<
         return it->second;
     float best = 1e30f;
     int choice = 0;
-    const int nvar = (c->L.Nx % 32 == 0) ? 3 : 2;
-    for (int v = 0; v < nvar; ++v)
+    for (int v = 0; v < 4; ++v)
     {
+        if ((v == 2 && c->L.Nx % 32 != 0) || (v == 3 && !sweep_ok(c->L)))
+            continue;
         launch_dirac<R>(c, v, false, nrhs, conf_d, conf0, in, out, U);  // warm-up
         cudaEventRecord(c->ev0, c->stream);
         for (int k = 0; k < 2; ++k)
@@ -300,7 +356,9 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     d.eigen_rule = eigen_rule;
     d.delta = 0.1;
     d.stall_limit = 3;
-    d.ru_period = mixed ? kRuPeriod : 1;
+    // batching reliable updates pays when right-hand sides would otherwise
+    // trigger them on different iterations; a single one only waits longer
+    d.ru_period = (mixed && nrhs > 1) ? kRuPeriod : 1;
     d.out_iters = c->w_iters;
     d.out_relres = c->w_relres;
     d.out_status = c->w_status;
@@ -833,11 +891,20 @@ uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
 
 int dwf_set_dslash_variant(dwf_ctx* c, int variant)
 {
-    if (!c || variant < -1 || variant > 2)
+    if (!c || variant < -1 || variant > 3)
         return DWF_BAD_ARG;
     c->dslash_variant = variant;
     if (variant == -1)
         c->dslash_tuned.clear();
+    return DWF_OK;
+}
+
+int dwf_set_dslash_chunk(dwf_ctx* c, int rows)
+{
+    if (!c || rows < 0)
+        return DWF_BAD_ARG;
+    c->dslash_chunk = rows;
+    c->dslash_tuned.clear();
     return DWF_OK;
 }
 

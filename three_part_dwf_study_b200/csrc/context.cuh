@@ -26,6 +26,8 @@ struct dwf_ctx
     // thread per 4-D site sweeping the fifth dimension; tuned choices cached
     // per (precision, batch-size bucket).
     int dslash_variant = -1;
+    int dslash_chunk = 0;    // rows per chunk of the t-sweeping Dslash (0 = automatic)
+    int sweep_smem_set = 0;  // t-sweeping kernels whose shared-memory limit is raised (bits)
     std::map<int, int> dslash_tuned;
     // CUDA events bracketing each persistent solver launch on `stream`
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -128,7 +128,7 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
         d.maxiter = maxiter;
         d.delta = 0.1;
         d.stall_limit = 3;
-        d.ru_period = kRuPeriod;
+        d.ru_period = d.nrhs > 1 ? kRuPeriod : 1;   // batching pays only across right-hand sides
         d.out_iters = c->w_iters;
         d.out_relres = c->w_relres;
         d.out_status = c->w_status;

@@ -29,6 +29,26 @@ __global__ void dirac_col_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>*
                                  long fsz, const cplx<R>* __restrict__ U, long usz,
                                  const int* __restrict__ conf, int conf0);
 
+// Same operator, one thread per (s, x) sweeping a chunk of tc rows in t
+// through a ring of S shared-memory row slots filled by cp.async (grid:
+// Nx/(32 G) x ceil(Nt/tc) x nrhs, block (32, Ls, G), Nx % 32 == 0,
+// 32 Ls G <= 512, dynamic shared memory S * sweep_slot_bytes).
+constexpr int kSweepSlots64 = 5;
+constexpr int kSweepSlots32 = 7;
+
+// One ring slot: spinors [Ls][32 G + 2] (halo column each side), t links
+// [32 G], x links [32 G + 1] (left halo first), rounded up to 16 bytes.
+__host__ __device__ constexpr size_t sweep_slot_bytes(int Ls, int G, size_t csize)
+{
+    return ((size_t(2) * Ls * (32 * G + 2) + 64 * G + 1) * csize + 15) / 16 * 16;
+}
+
+template <bool DAG, typename R, int S>
+__global__ void dirac_sweep_kernel(Lat L, const cplx<R>* __restrict__ in,
+                                   cplx<R>* __restrict__ out, long fsz,
+                                   const cplx<R>* __restrict__ U, long usz,
+                                   const int* __restrict__ conf, int conf0, int tc);
+
 // Per-(rhs, chunk) partials of |b - D2 t|^2 and |b|^2 (true residual of A x = b
 // after t = D1 x).
 template <bool DAG>

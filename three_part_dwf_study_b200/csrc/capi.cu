@@ -155,12 +155,14 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
     const long fs = c->fsz();
     if (variant == 3 && sweep_ok(c->L))
     {
-        constexpr int S = sizeof(R) == 8 ? kSweepSlots64 : kSweepSlots32;
+        constexpr int NPG = sizeof(R) == 8 ? kSweepGroups64 : kSweepGroups32;
+        constexpr int RPS = sizeof(R) == 8 ? kSweepRows64 : kSweepRows32;
+        constexpr int S = sweep_ring_rows(NPG, RPS);
         const SweepShape sh = sweep_shape(c, nrhs, 1024);
         const dim3 grid(c->L.Nx / (32 * sh.g), (c->L.Nt + sh.tc - 1) / sh.tc, nrhs);
         const dim3 block(32, c->L.Ls, sh.g);
         const size_t smem = S * sweep_slot_bytes(c->L.Ls, sh.g, sizeof(cplx<R>));
-        auto kern = dag ? dirac_sweep_kernel<true, R, S> : dirac_sweep_kernel<false, R, S>;
+        auto kern = dag ? dirac_sweep_kernel<true, R, NPG, RPS> : dirac_sweep_kernel<false, R, NPG, RPS>;
         const int bit = (dag ? 1 : 0) + (sizeof(R) == 8 ? 2 : 0);
         if (!(c->sweep_smem_set & (1 << bit)))
         {

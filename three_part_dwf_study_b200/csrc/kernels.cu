@@ -152,22 +152,41 @@ __device__ __forceinline__ void cp_link(float2* d, const float2* g) { cp_async8(
 
 }  // namespace
 
+// o + a w and o + a (i w), one fused multiply-add per component
+template <typename T, typename R>
+__device__ __forceinline__ T caxpy(R a, T w, T o)
+{
+    return mkc(fma(a, w.x, o.x), fma(a, w.y, o.y));
+}
+template <typename T, typename R>
+__device__ __forceinline__ T caxpy_i(R a, T w, T o)
+{
+    return mkc(fma(-a, w.y, o.x), fma(a, w.x, o.y));
+}
+
 // One block per (t chunk, G tiles of 32 consecutive x, all Ls slices), one
 // thread per (s, x). The block streams the rows t0-1 .. t1 of its tile
-// through a ring of S shared-memory slots with cp.async (S-3 rows in flight
-// while a row is computed; no registers held for them): a slot holds the
-// row's spinors for every s with one halo column on each side, and its t and
-// x links. Each thread keeps its own rows t-1, t, t+1 in registers and reads
-// the x +- 1 and s +- 1 neighbours and the links from the slot of row t. One
-// barrier per row. Every input spinor is loaded once per chunk (plus the two
-// halo rows and the two halo columns).
-template <bool DAG, typename R, int S>
+// through a ring of (NPG + 1) * RPS shared-memory row slots with cp.async, in
+// groups of RPS rows (NPG - 1 groups in flight while RPS rows are computed;
+// no registers held for them): a slot holds the row's spinors for every s
+// with one halo column on each side, and its t and x links. Each step a
+// thread computes RPS consecutive rows of its own (s, x) from a register
+// window of rows t-1 .. t+RPS, with the x +- 1 and s +- 1 neighbours and the
+// links read from the slot of the row; one barrier per step. Every input
+// spinor is loaded once per chunk (plus the two halo rows and columns). The
+// boundary signs and the -1/2 of the hopping term are folded into the
+// accumulation coefficients (one fused multiply-add per component and hop).
+template <bool DAG, typename R, int NPG, int RPS>
 __global__ void __launch_bounds__(512, 2)
     dirac_sweep_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
                        long fsz, const cplx<R>* __restrict__ U, long usz,
                        const int* __restrict__ conf, int conf0, int tc)
 {
-    static_assert(S >= 4, "the ring holds rows t-1, t, t+1 and the slot being refilled");
+    static_assert(RPS >= 1 && RPS <= 2, "one or two rows per step");
+    // rows needed by step q end in group q + A; the pending-group count must be >= 0
+    constexpr int A = (RPS + 1) / RPS;
+    static_assert(NPG - 1 - A >= 0, "prologue too short for the rows a step needs");
+    constexpr int NS = (NPG + 1) * RPS;                  // row slots in the ring
     using T = cplx<R>;
     extern __shared__ __align__(16) unsigned char sweep_smem[];
     const int j = blockIdx.z;
@@ -188,129 +207,175 @@ __global__ void __launch_bounds__(512, 2)
     const int own = s * W + i;
     const int sup = (s + 1 == Ls) ? 0 : s + 1;
     const int sdn = (s == 0) ? Ls - 1 : s - 1;
-    const int off_up = sup * W + i, off_dn = sdn * W + i;
+    // fifth-dimension sources of spin 1 and spin 0 (D: s+1 and s-1; D^dag: swapped)
+    const int off_s1 = (DAG ? sdn : sup) * W + i;
+    const int off_s0 = (DAG ? sup : sdn) * W + i;
     const int slot_c = int(sweep_slot_bytes(Ls, G, sizeof(T)) / sizeof(T));  // complex per slot
+    const int ring_c = NS * slot_c;
     T* const ring = reinterpret_cast<T*>(sweep_smem);
-    const int lk = 2 * plane;                            // links after the spinors
+    const int lt = 2 * plane + i - 1;                    // t link of this column
+    const int lx = 2 * plane + 32 * G + i;               // x link; lx - 1 is the one at x - 1
 
-    // this thread's input column (s, x) at row 0, its halo columns
-    const T* __restrict__ gin = in + j * fsz + 2 * (long(s) * V + x);
-    const T* __restrict__ gxl = in + j * fsz + 2 * (long(s) * V + xl);
-    const T* __restrict__ gxr = in + j * fsz + 2 * (long(s) * V + xr);
     const bool halo_l = (g == 0 && lane == 0), halo_r = (g == G - 1 && lane == 31);
+    const bool extra = halo_l || halo_r || s == 0;      // copies more than its own spinor
     const long rstride = 2L * Nx;                        // complex numbers per row
 
-    // row r of the chunk (t = t0 - 1 + r, wrapped) into slot `sl`; one commit
-    // group per row, empty past the last row so that the group count per step
-    // stays fixed
-    auto issue = [&](int r, int sl) {
-        if (r < nrow)
+    // Fetch state: the next chunk row (ri, at t = ti) with running pointers to
+    // this thread's spinor and links in that row; halo columns are fixed
+    // offsets from them.
+    int ri = 0;
+    int ti = (t0 == 0) ? Nt - 1 : t0 - 1;
+    const T* gp = in + j * fsz + 2 * (long(s) * V + long(ti) * Nx + x);
+    const T* up = Uj + ti * Nx + x;                      // t link; the x link is up + V
+    const long hl = 2L * (xl - x), hr = 2L * (xr - x);
+    const int ul = xl - x;
+    int bf = 0;                                          // slot (complex offset) of the next row
+
+    auto fetch_row = [&]() {
+        if (ri < nrow)
         {
-            int t = t0 - 1 + r;
-            t = (t < 0) ? t + Nt : ((t >= Nt) ? t - Nt : t);
-            T* const d = ring + sl * slot_c;
-            const long ro = t * rstride;
-            cp_slot_spinor(d, own, plane, gin + ro);
-            if (halo_l)
-                cp_slot_spinor(d, own - 1, plane, gxl + ro);
-            if (halo_r)
-                cp_slot_spinor(d, own + 1, plane, gxr + ro);
-            if (s == 0)
+            T* const d = ring + bf;
+            cp_slot_spinor(d, own, plane, gp);
+            if (extra)
             {
-                cp_link(d + lk + i - 1, Uj + t * Nx + x);
-                cp_link(d + lk + 32 * G + i, Uj + V + t * Nx + x);
                 if (halo_l)
-                    cp_link(d + lk + 32 * G, Uj + V + t * Nx + xl);
+                    cp_slot_spinor(d, own - 1, plane, gp + hl);
+                if (halo_r)
+                    cp_slot_spinor(d, own + 1, plane, gp + hr);
+                if (s == 0)
+                {
+                    cp_link(d + lt, up);
+                    cp_link(d + lx, up + V);
+                    if (halo_l)
+                        cp_link(d + lx - 1, up + V + ul);
+                }
             }
-        }
-        cp_async_commit();
-    };
-
-    const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
-    const R sxm = (x == 0) ? R(L.bcx) : R(1);
-    constexpr R kf = DAG ? R(1) : R(-1);
-    constexpr R kb = -kf;
-    const R dg = R(L.diag);
-    const R cup = (s + 1 == Ls) ? R(L.mf) : R(-1);
-    const R cdn = (s == 0) ? R(L.mf) : R(-1);
-    T* __restrict__ ocol = out + j * fsz + 2 * (long(s) * V + x);
-
-    for (int r = 0; r < S - 1; ++r)
-        issue(r, r);
-    // slots of rows k+1 (t), k+2 (t+1) and of the row being refilled (k-1)
-    int sc = 1, sn = 2, sf = S - 1;
-    Spinor<R> prev = {}, cur = {};
-    T Utm = {};
-    for (int k = 0; t0 + k < t1; ++k)
-    {
-        // rows k, k+1, k+2 (t-1, t, t+1) complete for every thread
-        cp_async_wait<S - 4>();
-        __syncthreads();
-        issue(k + S - 1, sf);   // the slot of row k-1, which no thread reads any more
-        const int t = t0 + k;
-        const T* const pc = ring + sc * slot_c;
-        if (k == 0)
-        {
-            prev = ld_slot_spinor(ring, own, plane);
-            cur = ld_slot_spinor(pc, own, plane);
-            Utm = ring[lk + i - 1];
-        }
-        const Spinor<R> next = ld_slot_spinor(ring + sn * slot_c, own, plane);
-        const Spinor<R> vxp = ld_slot_spinor(pc, own + 1, plane);
-        const Spinor<R> vxm = ld_slot_spinor(pc, own - 1, plane);
-        const T Ut = pc[lk + i - 1];
-        const T Ux = pc[lk + 32 * G + i];
-        const T Uxm = pc[lk + 32 * G + i - 1];
-        const R stp = (t == Nt - 1) ? R(L.bct) : R(1);
-        const R stm = (t == 0) ? R(L.bct) : R(1);
-
-        T w = cmul(Ut, stp * (next.s0 + kf * next.s1));
-        T hu = w;
-        T hl = kf * w;
-        w = cmulc(Utm, stm * (prev.s0 + kb * prev.s1));
-        hu += w;
-        hl += kb * w;
-        w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
-        hu += w;
-        hl += kf * itimes(w);
-        w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
-        hu += w;
-        hl += kb * itimes(w);
-        Spinor<R> o{dg * cur.s0 - R(0.5) * hu, dg * cur.s1 - R(0.5) * hl};
-        if (L.fifth)
-        {
-            // D: spin 1 from s+1 (m_f psi(0) at the top), spin 0 from s-1 (m_f psi(Ls-1) at 0);
-            // D^dag: the directions swapped.
-            if (!DAG)
+            ++ri;
+            if (++ti == Nt)
             {
-                o.s1 += cup * ld_slot_s1(pc, off_up, plane);
-                o.s0 += cdn * ld_slot_s0(pc, off_dn, plane);
+                ti = 0;
+                gp -= (Nt - 1) * rstride;
+                up -= (Nt - 1) * Nx;
             }
             else
             {
-                o.s1 += cdn * ld_slot_s1(pc, off_dn, plane);
-                o.s0 += cup * ld_slot_s0(pc, off_up, plane);
+                gp += rstride;
+                up += Nx;
             }
         }
-        st_spinor(ocol + t * rstride, 0, o);
-        prev = cur;
-        cur = next;
-        Utm = Ut;
-        sc = (sc + 1 == S) ? 0 : sc + 1;
-        sn = (sn + 1 == S) ? 0 : sn + 1;
-        sf = (sf + 1 == S) ? 0 : sf + 1;
+        bf = (bf + slot_c == ring_c) ? 0 : bf + slot_c;
+    };
+    // one commit group of RPS rows, empty past the last row so that the
+    // group count per step stays fixed
+    auto fetch_group = [&]() {
+        for (int d = 0; d < RPS; ++d)
+            fetch_row();
+        cp_async_commit();
+    };
+
+    const R half = R(0.5);
+    const R cbt = -half * R(L.bct);                      // -1/2 times the t boundary sign
+    constexpr R kf = DAG ? R(1) : R(-1);
+    constexpr R kb = -kf;
+    const R cxp = (x == Nx - 1) ? -half * R(L.bcx) : -half;
+    const R cxm = (x == 0) ? -half * R(L.bcx) : -half;
+    const R dg = R(L.diag);
+    // D: spin 1 from s+1 (m_f psi(0) at the top), spin 0 from s-1 (m_f psi(Ls-1) at 0);
+    // D^dag: the directions swapped.
+    const R c5_1 = DAG ? ((s == 0) ? R(L.mf) : R(-1)) : ((s + 1 == Ls) ? R(L.mf) : R(-1));
+    const R c5_0 = DAG ? ((s + 1 == Ls) ? R(L.mf) : R(-1)) : ((s == 0) ? R(L.mf) : R(-1));
+    T* __restrict__ op = out + j * fsz + 2 * (long(s) * V + long(t0) * Nx + x);
+
+    // output of row t from its slot pc, the rows t-1, t, t+1 of this column and
+    // the backward t link
+    auto site = [&](const T* pc, const Spinor<R>& pv, const Spinor<R>& cu, const Spinor<R>& nx,
+                    const T& Utm, int t) {
+        const Spinor<R> vxp = ld_slot_spinor(pc, own + 1, plane);
+        const Spinor<R> vxm = ld_slot_spinor(pc, own - 1, plane);
+        const T Ut = pc[lt];
+        const T Ux = pc[lx];
+        const T Uxm = pc[lx - 1];
+        const R ctp = (t == Nt - 1) ? cbt : -half;
+        const R ctm = (t == 0) ? cbt : -half;
+        Spinor<R> o{dg * cu.s0, dg * cu.s1};
+        T w = cmul(Ut, nx.s0 + kf * nx.s1);
+        o.s0 = caxpy(ctp, w, o.s0);
+        o.s1 = caxpy(kf * ctp, w, o.s1);
+        w = cmulc(Utm, pv.s0 + kb * pv.s1);
+        o.s0 = caxpy(ctm, w, o.s0);
+        o.s1 = caxpy(kb * ctm, w, o.s1);
+        w = cmul(Ux, vxp.s0 - kf * itimes(vxp.s1));
+        o.s0 = caxpy(cxp, w, o.s0);
+        o.s1 = caxpy_i(kf * cxp, w, o.s1);
+        w = cmulc(Uxm, vxm.s0 - kb * itimes(vxm.s1));
+        o.s0 = caxpy(cxm, w, o.s0);
+        o.s1 = caxpy_i(kb * cxm, w, o.s1);
+        if (L.fifth)
+        {
+            o.s1 = caxpy(c5_1, ld_slot_s1(pc, off_s1, plane), o.s1);
+            o.s0 = caxpy(c5_0, ld_slot_s0(pc, off_s0, plane), o.s0);
+        }
+        return o;
+    };
+    auto slot_at = [&](int b, int d) {   // slot d rows after slot b
+        const int o = b + d * slot_c;
+        return (o >= ring_c) ? o - ring_c : o;
+    };
+
+    for (int q = 0; q < NPG; ++q)
+        fetch_group();
+    // b0: slot of row t-1 for the first output row t of the step
+    int b0 = 0;
+    Spinor<R> prev = {}, cur = {};
+    T Utm = {};
+    for (int t = t0; t < t1; t += RPS)
+    {
+        // the rows t-1 .. t+RPS are complete for every thread
+        cp_async_wait<NPG - 1 - A>();
+        __syncthreads();
+        fetch_group();   // into the slots of the previous step's first rows
+        const T* const p1 = ring + slot_at(b0, 1);
+        if (t == t0)
+        {
+            prev = ld_slot_spinor(ring, own, plane);
+            cur = ld_slot_spinor(p1, own, plane);
+            Utm = ring[lt];
+        }
+        const Spinor<R> n1 = ld_slot_spinor(ring + slot_at(b0, 2), own, plane);
+        st_spinor(op, 0, site(p1, prev, cur, n1, Utm, t));
+        op += rstride;
+        if (RPS == 2)
+        {
+            const T Ut = p1[lt];
+            if (t + 1 < t1)
+            {
+                const T* const p2 = ring + slot_at(b0, 2);
+                const Spinor<R> n2 = ld_slot_spinor(ring + slot_at(b0, 3), own, plane);
+                st_spinor(op, 0, site(p2, cur, n1, n2, Ut, t + 1));
+                op += rstride;
+                Utm = p2[lt];
+                prev = n1;
+                cur = n2;
+            }
+        }
+        else
+        {
+            Utm = p1[lt];
+            prev = cur;
+            cur = n1;
+        }
+        b0 = slot_at(b0, RPS);
     }
     cp_async_wait<0>();
 }
 
-#define DWFB_SWEEP_INST(DAG, R, S)                                                               \
-    template __global__ void dirac_sweep_kernel<DAG, R, S>(Lat, const cplx<R>*, cplx<R>*, long, \
-                                                           const cplx<R>*, long, const int*, int,  \
-                                                           int);
-DWFB_SWEEP_INST(false, double, kSweepSlots64)
-DWFB_SWEEP_INST(true, double, kSweepSlots64)
-DWFB_SWEEP_INST(false, float, kSweepSlots32)
-DWFB_SWEEP_INST(true, float, kSweepSlots32)
+#define DWFB_SWEEP_INST(DAG, R, NPG, RPS)                                                         \
+    template __global__ void dirac_sweep_kernel<DAG, R, NPG, RPS>(                                \
+        Lat, const cplx<R>*, cplx<R>*, long, const cplx<R>*, long, const int*, int, int);
+DWFB_SWEEP_INST(false, double, kSweepGroups64, kSweepRows64)
+DWFB_SWEEP_INST(true, double, kSweepGroups64, kSweepRows64)
+DWFB_SWEEP_INST(false, float, kSweepGroups32, kSweepRows32)
+DWFB_SWEEP_INST(true, float, kSweepGroups32, kSweepRows32)
 #undef DWFB_SWEEP_INST
 
 template __global__ void dirac_kernel<false, double>(Lat, const double2*, double2*, long,

@@ -29,12 +29,14 @@ __global__ void dirac_col_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>*
                                  long fsz, const cplx<R>* __restrict__ U, long usz,
                                  const int* __restrict__ conf, int conf0);
 
-// Same operator, one thread per (s, x) sweeping a chunk of tc rows in t
-// through a ring of S shared-memory row slots filled by cp.async (grid:
-// Nx/(32 G) x ceil(Nt/tc) x nrhs, block (32, Ls, G), Nx % 32 == 0,
-// 32 Ls G <= 512, dynamic shared memory S * sweep_slot_bytes).
-constexpr int kSweepSlots64 = 5;
-constexpr int kSweepSlots32 = 7;
+// Same operator, one thread per (s, x) sweeping a chunk of tc rows in t,
+// RPS rows per step, through a ring of (NPG + 1) * RPS shared-memory row
+// slots filled by cp.async (grid: Nx/(32 G) x ceil(Nt/tc) x nrhs, block
+// (32, Ls, G), Nx % 32 == 0, 32 Ls G <= 512, dynamic shared memory
+// (NPG + 1) * RPS * sweep_slot_bytes).
+constexpr int kSweepRows64 = 1, kSweepGroups64 = 4;   // two FP64 rows per step spill at 64 registers
+constexpr int kSweepRows32 = 2, kSweepGroups32 = 3;
+constexpr int sweep_ring_rows(int npg, int rps) { return (npg + 1) * rps; }
 
 // One ring slot: spinors [Ls][32 G + 2] (halo column each side), t links
 // [32 G], x links [32 G + 1] (left halo first), rounded up to 16 bytes.
@@ -43,7 +45,7 @@ __host__ __device__ constexpr size_t sweep_slot_bytes(int Ls, int G, size_t csiz
     return ((size_t(2) * Ls * (32 * G + 2) + 64 * G + 1) * csize + 15) / 16 * 16;
 }
 
-template <bool DAG, typename R, int S>
+template <bool DAG, typename R, int NPG, int RPS>
 __global__ void dirac_sweep_kernel(Lat L, const cplx<R>* __restrict__ in,
                                    cplx<R>* __restrict__ out, long fsz,
                                    const cplx<R>* __restrict__ U, long usz,

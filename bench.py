@@ -338,22 +338,24 @@ def impl_reference(args):
 HMC_EPS, HMC_STEPS = 0.01, 40  # the reference's dwf.epsilon and dwf.leapfrog_steps
 
 
-def hmc_compare(T, d, rank, ntraj):
-    """ntraj domain-wall HMC trajectories from the workload configuration, each
-    run twice from identical momenta and pseudofermion draws (libstdc++
-    streams, the reference's order: chi then pi): pseudofermion solves by the
-    plain FP64 CG and by the mixed CG, both to 1e-10. Reports device time per
-    trajectory (CUDA events on the library stream around the whole
-    trajectory), dH of each and their largest difference, and the plaquette."""
+def hmc_compare(T, d, rank, ntraj, theta=None, lattice=None, seed=1234, maxiter=MAXITER):
+    """ntraj domain-wall HMC trajectories from `theta` (default: the workload
+    configuration), each run twice from identical momenta and pseudofermion
+    draws (libstdc++ streams, the reference's order: chi then pi):
+    pseudofermion solves by the plain FP64 CG and by the mixed CG, both to
+    1e-10. Reports device time per trajectory (CUDA events on the library
+    stream around the whole trajectory), dH of each and their largest
+    difference, and the plaquette."""
     import torch
     from three_part_dwf_study_b200.rng import Rng
     if ntraj < 1:
         return None
     stream = torch.cuda.ExternalStream(d.stream_ptr())
-    theta = workload_gauge(rank)
-    rng = Rng(1234 + rank)
-    res = {"lattice": [NT, NX, LS], "epsilon": HMC_EPS, "leapfrog_steps": HMC_STEPS,
-           "rtol": RTOL, "trajectories": ntraj}
+    if theta is None:
+        theta = workload_gauge(rank)
+    rng = Rng(seed + rank)
+    res = {"lattice": list(lattice or (NT, NX, LS)), "epsilon": HMC_EPS,
+           "leapfrog_steps": HMC_STEPS, "rtol": RTOL, "trajectories": ntraj}
     per = {T.SOLVER_CG64: [], T.SOLVER_MIXED: []}
     dh = {T.SOLVER_CG64: [], T.SOLVER_MIXED: []}
     plaq = []
@@ -367,7 +369,7 @@ def hmc_compare(T, d, rank, ntraj):
             torch.cuda.synchronize()
             e0.record(stream)
             out, info = d.hmc_trajectory(theta, chi, mom, HMC_EPS, HMC_STEPS, rtol=RTOL,
-                                         maxiter=MAXITER, solver=solver)
+                                         maxiter=maxiter, solver=solver)
             e1.record(stream)
             e1.synchronize()
             per[solver].append(e0.elapsed_time(e1) * 1e-3)
@@ -384,6 +386,29 @@ def hmc_compare(T, d, rank, ntraj):
         res["mixed_cg"]["seconds_per_trajectory"]
     res["plaquette"] = plaq
     return res
+
+
+# DWF 128x128, Ls = 24, M5 = 1, m_f = 0.02, beta = 4: the larger HMC comparison
+C5_LATTICE, C5_M5, C5_MF, C5_BETA = (128, 128, 24), 1.0, 0.02, 4.0
+
+
+def hmc_compare_large(T, local, ntraj):
+    """The same FP64-vs-mixed HMC comparison on DWF 128x128, Ls = 24,
+    m_f = 0.02 from a seeded beta = 4 start (a bounded sample of trajectories;
+    the study runs 200)."""
+    from three_part_dwf_study_b200.ensemble import quenched_theta
+    if ntraj < 1:
+        return None
+    Nt, Nx, Ls = C5_LATTICE
+    d = T.DomainWall(Nt, Nx, Ls, C5_M5, C5_MF, C5_BETA, device=local)
+    theta = quenched_theta(np.random.default_rng(GAUGE_SEED + 5), Nt, Nx, C5_BETA)
+    try:
+        res = hmc_compare(T, d, 0, ntraj, theta=theta, lattice=C5_LATTICE, seed=4321,
+                          maxiter=50000)
+        res.update({"M5": C5_M5, "mf": C5_MF, "beta": C5_BETA})
+        return res
+    finally:
+        d.close()
 
 
 def wilson_learned_grid(T, ntrain=8):
@@ -630,6 +655,7 @@ def impl_ours(args):
 
     # ---- HMC on the same lattice: FP64 and mixed CG on the same trajectories ----
     hmc = hmc_compare(T, d, rank, args.hmc_trajectories)
+    hmc_large = hmc_compare_large(T, local, args.hmc_large_trajectories) if ws == 1 else None
     # ---- Wilson 64x64 near the critical mass with the learned preconditioner ----
     wil = wilson_learned_grid(T) if (args.wilson_learned and ws == 1) else None
 
@@ -712,6 +738,7 @@ def impl_ours(args):
         "roofline": roofline,
         "dslash": dslash,
         "hmc": hmc,
+        "hmc_128x128x24": hmc_large,
         "learned_wilson_64x64": wil,
         "gpu_launches": launches,
         "clocks": clocks,
@@ -886,6 +913,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
+    ap.add_argument("--hmc-large-trajectories", type=int, default=1,
+                    help="HMC trajectories of the 128x128x24 FP64-vs-mixed comparison (0: skip)")
     ap.add_argument("--hmc-trajectories", type=int, default=2,
                     help="HMC trajectories compared between FP64 and mixed CG (0: skip)")
     ap.add_argument("--no-wilson-learned", dest="wilson_learned", action="store_false",

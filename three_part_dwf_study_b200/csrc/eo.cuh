@@ -88,6 +88,58 @@ __device__ __forceinline__ Spinor<R> eo_hop(const Ld& in, const cplx<R>* __restr
     return {R(-0.5) * up, R(-0.5) * lo};
 }
 
+// eo_hop at a fixed 4-D site for any slice: the neighbour offsets within a
+// parity slice and the four links (boundary signs folded in, exact for signs
+// +-1) are computed once, so a loop over the Ls slices only loads spinors.
+template <bool DAG, typename R>
+struct EoHopSite
+{
+    cplx<R> ut, utm, ux, uxm;
+    int otp, otm, oxp, oxm;
+    __device__ __forceinline__ EoHopSite(const cplx<R>* __restrict__ U, const Lat& L, EoGeo g,
+                                         int t, int x)
+    {
+        const int Nt = L.Nt, Nx = L.Nx;
+        const int tp = (t + 1 == Nt) ? 0 : t + 1;
+        const int tm = (t == 0) ? Nt - 1 : t - 1;
+        const int xp = (x + 1 == Nx) ? 0 : x + 1;
+        const int xm = (x == 0) ? Nx - 1 : x - 1;
+        otp = tp * g.Nxh + (x >> 1);
+        otm = tm * g.Nxh + (x >> 1);
+        oxp = t * g.Nxh + (xp >> 1);
+        oxm = t * g.Nxh + (xm >> 1);
+        const int here = t * Nx + x;
+        ut = ((t == Nt - 1) ? R(L.bct) : R(1)) * U[here];
+        utm = ((t == 0) ? R(L.bct) : R(1)) * U[tm * Nx + x];
+        ux = ((x == Nx - 1) ? R(L.bcx) : R(1)) * U[L.V + here];
+        uxm = ((x == 0) ? R(L.bcx) : R(1)) * U[L.V + t * Nx + xm];
+    }
+    template <typename Ld>
+    __device__ __forceinline__ Spinor<R> at(const Ld& in, long sb) const
+    {
+        using T = cplx<R>;
+        constexpr R kf = DAG ? R(1) : R(-1);
+        constexpr R kb = -kf;
+        const Spinor<R> vtp = in.sp(sb + otp);
+        const Spinor<R> vtm = in.sp(sb + otm);
+        const Spinor<R> vxp = in.sp(sb + oxp);
+        const Spinor<R> vxm = in.sp(sb + oxm);
+        T w = cmul(ut, vtp.s0 + kf * vtp.s1);
+        T up = w;
+        T lo = kf * w;
+        w = cmulc(utm, vtm.s0 + kb * vtm.s1);
+        up += w;
+        lo += kb * w;
+        w = cmul(ux, vxp.s0 - kf * itimes(vxp.s1));
+        up += w;
+        lo += kf * itimes(w);
+        w = cmulc(uxm, vxm.s0 - kb * itimes(vxm.s1));
+        up += w;
+        lo += kb * itimes(w);
+        return {R(-0.5) * up, R(-0.5) * lo};
+    }
+};
+
 // M5 (DAG = false) or M5^dag at slice s of the 4-D site h of a parity field.
 template <bool DAG, typename R, typename Ld>
 __device__ __forceinline__ Spinor<R> eo_m5(const Ld& in, const Lat& L, EoGeo g, int s, int h)
@@ -202,9 +254,12 @@ __device__ __forceinline__ void eo_hopinv_site_smem(const Ld& in, cplx<R>* __res
     T s_up = mkc(R(0), R(0)), s_dn = mkc(R(0), R(0));
     R pw = ci;
     R cmls = R(1);
+    const EoHopSite<DAG, R> hs(U, L, g, t, x);
+    // unrolled so that several slices' neighbour loads are in flight together
+#pragma unroll 4
     for (int s = 0; s < Ls; ++s)
     {
-        const Spinor<R> hv = eo_hop<DAG, R>(in, U, L, g, s, t, x);
+        const Spinor<R> hv = hs.at(in, long(s) * g.Vh);
         zs[s * zstride] = hv;
         const T zu = DAG ? hv.s0 : hv.s1;
         const T zd = DAG ? hv.s1 : hv.s0;

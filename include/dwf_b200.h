@@ -431,9 +431,12 @@ int dwf_lp_train(dwf_ctx* ctx, const dwf_lp_train_params* params, dwf_lp_train_i
  * events around `reps` back-to-back applications on the context stream) and
  * its arithmetic: 8 * 9 * sum_l cin_l cout_l * V * nrhs real flops. */
 int dwf_lp_time_network(dwf_ctx* ctx, int nrhs, int reps, double* ms_per_apply, double* flops_per_apply);
-/* Layer kernel: -1 automatic (default: the tcgen05 kernel wherever its shared-
- * memory tile fits, else the mma.sync kernel), 0 the mma.sync kernel, 1 the
- * tcgen05 kernel only (DWF_BAD_ARG where it does not fit). */
+/* Layer kernel: -1 automatic (default: the first DWF_SOLVER_LEARNED solve per
+ * batch-size bucket times one network application with each kernel and keeps
+ * the faster; the tcgen05 kernel competes only where every layer's shared-
+ * memory tile fits; before any solve, the tcgen05 kernel wherever it fits),
+ * 0 the mma.sync kernel, 1 the tcgen05 kernel only (DWF_BAD_ARG where it does
+ * not fit). */
 int dwf_lp_set_variant(dwf_ctx* ctx, int variant);
 /* Inner solve: stop at |r| <= inner_tol |r0| or inner_maxiter iterations;
  * at most outer_max defect-correction cycles (defaults 1e-4, 400, 40). */

@@ -233,3 +233,29 @@ def test_learned_wilson(T):
         assert rel(x[k], x64[k]) < 1e-7
         assert info[k]["schur_iterations"] < i64[k]["iterations"]
     w.close()
+
+
+def test_learned_solve_kernel_choices_agree(T):
+    """The learned solve with the mma.sync layer kernel, the tcgen05 layer
+    kernel and the automatic choice (both timed at the first solve, the faster
+    kept): every result meets the stopping rule and equals the FP64 solution."""
+    rng = np.random.default_rng(9)
+    w = T.Wilson(16, 32, -0.02, 3.0)
+    th = np.stack([quenched_theta(rng, 16, 32, 3.0) for _ in range(2)])
+    w.set_gauge(th)
+    w.lp_init(hidden=8, seed=9)
+    w.lp_train(steps=300, batch=8, lr=3e-3, lr_decay_steps=150, pairs_per_conf=32,
+               solver_iters=20, seed=9)
+    src = np.zeros((3, w.Ndof), np.complex128)
+    for k in range(3):
+        src[k, 2 * (5 * k * 32 + k) + (k % 2)] = 1.0
+    conf = [0, 1, 0]
+    x64, _ = w.propagators(src, rhs_conf=conf, rtol=1e-12, maxiter=40000, solver=T.SOLVER_CG64)
+    for variant in (0, 1, -1, -1):
+        w.lp_set_variant(variant)
+        x, info = w.propagators(src, rhs_conf=conf, rtol=1e-10, maxiter=20000,
+                                solver=T.SOLVER_LEARNED)
+        for k in range(3):
+            assert info[k]["converged"] and info[k]["true_relres"] <= 1e-10, (variant, info[k])
+            assert rel(x[k], x64[k]) < 1e-7, variant
+    w.close()

@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <random>
 #include <string>
 #include <vector>
@@ -1608,6 +1609,8 @@ struct LpNet
     long tf_off[kLpLayers + 1], ta_off[kLpLayers + 1];
     int ncf[kLpLayers], nca[kLpLayers];
     int variant = -1;                  // -1 auto, 0 mma.sync kernel, 1 tcgen05 kernel
+    int auto_variant = -1;             // the automatic choice in force (-1: tcgen05 where it fits)
+    std::map<int, int> auto_tuned;     // automatic choice per batch-size bucket
     int* err_d = nullptr;              // bounded-wait error flag of the tcgen05 kernel
     float2* T = nullptr;               // transports [nconf][V][9]
     int T_cap = 0;
@@ -1769,6 +1772,9 @@ FieldLayout op_layout(const dwf_ctx* c)
 
 FieldLayout net_layout(const dwf_ctx* c, int C) { return FieldLayout{long(c->L.V) * C, C, C, 0}; }
 
+// The layer kernel choice in force: the explicit setting, else the automatic one.
+int lp_eff_variant(const LpNet* n) { return n->variant >= 0 ? n->variant : n->auto_variant; }
+
 // Whether the tcgen05 kernel takes layer l (its shared-memory tile fits).
 bool tc_fits(const dwf_ctx* c, int l, bool adjoint)
 {
@@ -1791,7 +1797,7 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
     const int ncol = ncol_of(co);
     const size_t tsm = tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx);
     const bool tc_ok = tc_fits(c, l, adjoint);
-    if (n->variant != 0 && tc_ok)
+    if (lp_eff_variant(n) != 0 && tc_ok)
     {
         TcArgs t;
         t.in = in;
@@ -1898,7 +1904,7 @@ int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* 
     LpNet* n = c->lp;
     ST(lp_ensure_act(c, nrhs));
     const FieldLayout lop = op_layout(c), lh = net_layout(c, n->H);
-    bool chain = !keep && n->variant != 0;
+    bool chain = !keep && lp_eff_variant(n) != 0;
     for (int l = 0; l < kLpLayers; ++l)
         chain = chain && tc_fits(c, l, adjoint);
     if (chain)
@@ -1942,7 +1948,7 @@ int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* 
 // Whether lp_net runs the tcgen05 chain with BF16 planar activations.
 bool lp_chain(const dwf_ctx* c, bool adjoint)
 {
-    bool chain = c->lp->variant != 0;
+    bool chain = lp_eff_variant(c->lp) != 0;
     for (int l = 0; l < kLpLayers; ++l)
         chain = chain && tc_fits(c, l, adjoint);
     return chain;
@@ -2118,6 +2124,57 @@ void lp_destroy(dwf_ctx* c)
 // Solve D x = src for nrhs sources: FP64 defect correction around an FP32
 // BiCGStab inner solve right-preconditioned by the network, then (for right-
 // hand sides that stall) the mixed CG on D^dag D from the current iterate.
+// Automatic layer kernel (variant -1): the first solve per batch-size bucket
+// times one network application with each kernel (CUDA events, after a
+// warm-up) and keeps the faster; the tcgen05 kernel competes only where every
+// layer's tile fits. Uses the solver's scratch fields.
+int lp_tune_variant(dwf_ctx* c, int nrhs, const int* conf_d)
+{
+    LpNet* n = c->lp;
+    int bucket = 0;
+    while ((1 << bucket) < nrhs && bucket < 20)
+        ++bucket;
+    const auto it = n->auto_tuned.find(bucket);
+    if (it != n->auto_tuned.end())
+    {
+        n->auto_variant = it->second;
+        return DWF_OK;
+    }
+    bool tc_all = true;
+    for (int l = 0; l < kLpLayers; ++l)
+        tc_all = tc_all && tc_fits(c, l, false) && tc_fits(c, l, true);
+    int choice = 0;
+    if (tc_all)
+    {
+        const long nf = long(nrhs) * c->fsz();
+        ST(lp_gauss(c, n->s_r64, nf, 777));
+        lp_f64_to_f32_kernel<<<grid_for(nf, c->nsm), 256, 0, c->stream>>>(n->s_r64, n->s_f32[0], nf);
+        c->launches += 1;
+        float best = 1e30f;
+        for (int v = 0; v <= 1; ++v)
+        {
+            n->auto_variant = v;
+            ST(lp_net(c, false, nrhs, conf_d, n->s_f32[0], n->s_f32[1], false));  // warm-up
+            CK(cudaEventRecord(c->ev0, c->stream));
+            for (int r = 0; r < 3; ++r)
+                ST(lp_net(c, false, nrhs, conf_d, n->s_f32[0], n->s_f32[1], false));
+            CK(cudaEventRecord(c->ev1, c->stream));
+            CK(cudaEventSynchronize(c->ev1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            if (ms < best)
+            {
+                best = ms;
+                choice = v;
+            }
+        }
+        ST(lp_check_err(c));
+    }
+    n->auto_tuned[bucket] = choice;
+    n->auto_variant = choice;
+    return DWF_OK;
+}
+
 int lp_solve(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
              double rtol, int maxiter, dwf_solve_info* info)
 {
@@ -2133,6 +2190,8 @@ int lp_solve(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double
     // the fused update kernels write the network's planar input (hb[0]) before
     // the network runs: size the activation buffers for this batch first
     ST(lp_ensure_act(c, nrhs));
+    if (n->variant < 0)
+        ST(lp_tune_variant(c, nrhs, conf_d));
     const long fs = c->fsz();
     const long nf = fs * nrhs;
     const int nblk = int(std::min<long>(64, (fs + 4095) / 4096));
@@ -2253,7 +2312,7 @@ int lp_solve(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double
         // the first chunk runs directly (it also settles the Dslash autotuner)
         const std::vector<uintptr_t> key = {uintptr_t(nrhs), uintptr_t(chain), uintptr_t(n->s_rhs),
                                             uintptr_t(n->act_rhs), uintptr_t(n->T), uintptr_t(conf_d),
-                                            uintptr_t(c->U32), uintptr_t(n->variant),
+                                            uintptr_t(c->U32), uintptr_t(lp_eff_variant(n) + 1),
                                             uintptr_t(std::llround(std::log10(tgt2) * 1000.0)),
                                             uintptr_t(n->inner_max), uintptr_t(nblk), uintptr_t(c->dslash_variant)};
         for (int it = 0; it < n->inner_max; it += chunk)

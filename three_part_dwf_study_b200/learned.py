@@ -125,7 +125,8 @@ class LearnedMixin:
         return ms.value, fl.value
 
     def lp_set_variant(self, variant):
-        """Layer kernel: -1 automatic, 0 mma.sync, 1 tcgen05."""
+        """Layer kernel: -1 automatic (the first learned solve per batch size
+        times both kernels and keeps the faster), 0 mma.sync, 1 tcgen05."""
         self._check(A.lib().dwf_lp_set_variant(self._h, int(variant)))
 
     def lp_set_solver(self, inner_tol=1e-4, inner_maxiter=400, outer_max=40):

@@ -1611,6 +1611,8 @@ struct LpNet
     int variant = -1;                  // -1 auto, 0 mma.sync kernel, 1 tcgen05 kernel
     int auto_variant = -1;             // the automatic choice in force (-1: tcgen05 where it fits)
     std::map<int, int> auto_tuned;     // automatic choice per batch-size bucket
+    std::map<long, int> conv_bps;      // resident blocks per SM of the mma.sync kernel (nt, smem)
+    bool smem_set = false;             // layer kernels' shared-memory limit raised on this device
     int* err_d = nullptr;              // bounded-wait error flag of the tcgen05 kernel
     float2* T = nullptr;               // transports [nconf][V][9]
     int T_cap = 0;
@@ -1679,8 +1681,8 @@ int cpad_of(int c) { return (c + 7) / 8 * 8; }
 
 int set_conv_smem(dwf_ctx* c)
 {
-    static int done_dev = -1;
-    if (done_dev == c->device)
+    // per context (each context drives one device); the attribute is per device
+    if (c->lp->smem_set)
         return DWF_OK;
     const int mx = 220 * 1024;
     CK(cudaFuncSetAttribute(lp_conv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
@@ -1694,7 +1696,7 @@ int set_conv_smem(dwf_ctx* c)
     CK(cudaFuncSetAttribute(lp_tc_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     CK(cudaFuncSetAttribute(lp_tc_kernel<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    done_dev = c->device;
+    c->lp->smem_set = true;
     return DWF_OK;
 }
 
@@ -1775,6 +1777,14 @@ FieldLayout net_layout(const dwf_ctx* c, int C) { return FieldLayout{long(c->L.V
 // The layer kernel choice in force: the explicit setting, else the automatic one.
 int lp_eff_variant(const LpNet* n) { return n->variant >= 0 ? n->variant : n->auto_variant; }
 
+// Whether the tcgen05 kernel (and its BF16 planar chain) may run: chosen
+// explicitly, or automatic before any timing.
+bool lp_tc_allowed(const LpNet* n)
+{
+    const int v = lp_eff_variant(n);
+    return v == 1 || v == -1;
+}
+
 // Whether the tcgen05 kernel takes layer l (its shared-memory tile fits).
 bool tc_fits(const dwf_ctx* c, int l, bool adjoint)
 {
@@ -1797,7 +1807,7 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
     const int ncol = ncol_of(co);
     const size_t tsm = tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx);
     const bool tc_ok = tc_fits(c, l, adjoint);
-    if (lp_eff_variant(n) != 0 && tc_ok)
+    if (lp_tc_allowed(n) && tc_ok)
     {
         TcArgs t;
         t.in = in;
@@ -1858,18 +1868,31 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
     const int nt = nt_of(a.cout);
     const size_t smem = conv_smem_bytes(a.cpad, nt, a.tx);
     const long ntiles = long((a.Nt + kTileRows - 1) / kTileRows) * ((a.Nx + a.tx - 1) / a.tx) * nrhs;
-    const int grid = int(std::max<long>(1, std::min<long>(ntiles, 2L * c->nsm)));
     ST(set_conv_smem(c));
+    const void* fn = nullptr;
     switch (nt)
     {
-    case 1: lp_conv_kernel<1><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
-    case 2: lp_conv_kernel<2><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
-    case 4: lp_conv_kernel<4><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
-    case 6: lp_conv_kernel<6><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
-    case 8: lp_conv_kernel<8><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
-    case 12: lp_conv_kernel<12><<<grid, kConvWarps * 32, smem, c->stream>>>(a); break;
+    case 1: fn = reinterpret_cast<const void*>(&lp_conv_kernel<1>); break;
+    case 2: fn = reinterpret_cast<const void*>(&lp_conv_kernel<2>); break;
+    case 4: fn = reinterpret_cast<const void*>(&lp_conv_kernel<4>); break;
+    case 6: fn = reinterpret_cast<const void*>(&lp_conv_kernel<6>); break;
+    case 8: fn = reinterpret_cast<const void*>(&lp_conv_kernel<8>); break;
+    case 12: fn = reinterpret_cast<const void*>(&lp_conv_kernel<12>); break;
     default: return ctx_fail(c, DWF_BAD_ARG, "learned: unsupported channel count");
     }
+    // every block walks tiles in turn (stage, MMAs, transporters, store), so
+    // the tiles in flight per SM are the resident blocks: fill them all
+    const long key = long(nt) * (1L << 32) + long(smem);
+    auto it = n->conv_bps.find(key);
+    if (it == n->conv_bps.end())
+    {
+        int bps = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kConvWarps * 32, smem));
+        it = n->conv_bps.emplace(key, std::max(1, bps)).first;
+    }
+    const int grid = int(std::max<long>(1, std::min<long>(ntiles, long(it->second) * c->nsm)));
+    void* args[] = {&a};
+    CK(cudaLaunchKernel(fn, dim3(grid), dim3(kConvWarps * 32), args, smem, c->stream));
     c->launches += 1;
     CK(cudaGetLastError());
     return DWF_OK;
@@ -1904,7 +1927,7 @@ int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* 
     LpNet* n = c->lp;
     ST(lp_ensure_act(c, nrhs));
     const FieldLayout lop = op_layout(c), lh = net_layout(c, n->H);
-    bool chain = !keep && lp_eff_variant(n) != 0;
+    bool chain = !keep && lp_tc_allowed(n);
     for (int l = 0; l < kLpLayers; ++l)
         chain = chain && tc_fits(c, l, adjoint);
     if (chain)
@@ -1948,7 +1971,7 @@ int lp_net(dwf_ctx* c, bool adjoint, int nrhs, const int* conf_d, const float2* 
 // Whether lp_net runs the tcgen05 chain with BF16 planar activations.
 bool lp_chain(const dwf_ctx* c, bool adjoint)
 {
-    bool chain = lp_eff_variant(c->lp) != 0;
+    bool chain = lp_tc_allowed(c->lp);
     for (int l = 0; l < kLpLayers; ++l)
         chain = chain && tc_fits(c, l, adjoint);
     return chain;

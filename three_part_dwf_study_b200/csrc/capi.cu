@@ -131,11 +131,15 @@ struct SweepShape
 // the grid holds at least two blocks per resident slot (1024 resident threads
 // per SM, as the kernel's launch bounds allow), so the tail of the launch
 // stays short.
-SweepShape sweep_shape(const dwf_ctx* c, int nrhs, int resident_threads)
+// Largest dynamic shared memory of one block (the sweep's ring must fit).
+constexpr size_t kSweepSmemMax = 227 * 1024;
+
+SweepShape sweep_shape(const dwf_ctx* c, int nrhs, int resident_threads, int ring_rows, size_t csize)
 {
     const Lat& L = c->L;
     int g = 1;
-    while (32 * L.Ls * g * 2 <= 512 && (L.Nx / 32) % (g * 2) == 0)
+    while (32 * L.Ls * g * 2 <= 512 && (L.Nx / 32) % (g * 2) == 0 &&
+           ring_rows * sweep_slot_bytes(L.Ls, g * 2, csize) <= kSweepSmemMax)
         g *= 2;
     const long nxt = L.Nx / (32 * g);
     int tc = c->dslash_chunk > 0 ? std::min(c->dslash_chunk, L.Nt) : L.Nt;
@@ -158,7 +162,9 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
         constexpr int NPG = sizeof(R) == 8 ? kSweepGroups64 : kSweepGroups32;
         constexpr int RPS = sizeof(R) == 8 ? kSweepRows64 : kSweepRows32;
         constexpr int S = sweep_ring_rows(NPG, RPS);
-        const SweepShape sh = sweep_shape(c, nrhs, 1024);
+        // resident threads per SM as the kernel's launch bounds allow
+        const SweepShape sh = sweep_shape(c, nrhs, (sizeof(R) == 8 && RPS == 2) ? 512 : 1024, S,
+                                          sizeof(cplx<R>));
         const dim3 grid(c->L.Nx / (32 * sh.g), (c->L.Nt + sh.tc - 1) / sh.tc, nrhs);
         const dim3 block(32, c->L.Ls, sh.g);
         const size_t smem = S * sweep_slot_bytes(c->L.Ls, sh.g, sizeof(cplx<R>));
@@ -171,7 +177,11 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
             // cudaGetLastError check reports
             size_t most = 0;
             for (int g = 1; 32 * c->L.Ls * g <= 512; g *= 2)
-                most = std::max(most, S * sweep_slot_bytes(c->L.Ls, g, sizeof(cplx<R>)));
+            {
+                const size_t b = S * sweep_slot_bytes(c->L.Ls, g, sizeof(cplx<R>));
+                if (b <= kSweepSmemMax)
+                    most = std::max(most, b);
+            }
             if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(most)) ==
                 cudaSuccess)
                 c->sweep_smem_set |= 1 << bit;

@@ -177,7 +177,7 @@ __device__ __forceinline__ T caxpy_i(R a, T w, T o)
 // boundary signs and the -1/2 of the hopping term are folded into the
 // accumulation coefficients (one fused multiply-add per component and hop).
 template <bool DAG, typename R, int NPG, int RPS>
-__global__ void __launch_bounds__(512, 2)
+__global__ void __launch_bounds__(512, (sizeof(R) == 8 && RPS == 2) ? 1 : 2)
     dirac_sweep_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
                        long fsz, const cplx<R>* __restrict__ U, long usz,
                        const int* __restrict__ conf, int conf0, int tc)

@@ -34,7 +34,7 @@ __global__ void dirac_col_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>*
 // slots filled by cp.async (grid: Nx/(32 G) x ceil(Nt/tc) x nrhs, block
 // (32, Ls, G), Nx % 32 == 0, 32 Ls G <= 512, dynamic shared memory
 // (NPG + 1) * RPS * sweep_slot_bytes).
-constexpr int kSweepRows64 = 1, kSweepGroups64 = 4;   // two FP64 rows per step spill at 64 registers
+constexpr int kSweepRows64 = 1, kSweepGroups64 = 4;   // two FP64 rows per step need one block per SM: slower
 constexpr int kSweepRows32 = 2, kSweepGroups32 = 3;
 constexpr int sweep_ring_rows(int npg, int rps) { return (npg + 1) * rps; }
 

@@ -12,12 +12,18 @@ using namespace dwfb;
 
 // The even-odd path's Schur solve stops at this multiple of the requested
 // tolerance (on its own normal equation); the full-lattice mixed solve that
-// follows enforces the reference's rule on D^dag D. Measured on the
-// 64x64x16, 28-source propagator set (solves/s): 0.3 -> 737, 1 -> 759,
-// 2 -> 778, 3 -> 789-795, 4 -> 769, 5 -> 753, 10 -> 699: up to ~3 the check
-// finishes within its first reliable-update period (16 iterations).
+// follows, warm-started from it, enforces the reference's rule on D^dag D.
+// Warm-started batched mixed solves run FP64 reliable updates every
+// DWFB_RU_PERIOD_WARM iterations (a check that starts next to the solution
+// should not wait a full period). Measured on the 64x64x16, 28-source
+// propagator set (solves/s, warm period / factor): 16 / 0.3 -> 737,
+// 16 / 3 -> 789-795, 16 / 10 -> 699, 8 / 5 -> 780, 4 / 2.5 -> 818,
+// 4 / 3 -> 829, 4 / 4 -> 788, 4 / 6 -> 735, 2 / 3 -> 828, 2 / 4 -> 786.
 #ifndef DWFB_EO_SCHUR_TOL
 #define DWFB_EO_SCHUR_TOL 3.0
+#endif
+#ifndef DWFB_RU_PERIOD_WARM
+#define DWFB_RU_PERIOD_WARM 4
 #endif
 
 #define CK(call)                                                                        \
@@ -380,7 +386,7 @@ int launch_solver(dwf_ctx* c, bool mixed, int op, int nrhs, const double2* b, do
     d.stall_limit = 3;
     // batching reliable updates pays when right-hand sides would otherwise
     // trigger them on different iterations; a single one only waits longer
-    d.ru_period = (mixed && nrhs > 1) ? kRuPeriod : 1;
+    d.ru_period = (mixed && nrhs > 1) ? (has_guess ? DWFB_RU_PERIOD_WARM : kRuPeriod) : 1;
     d.out_iters = c->w_iters;
     d.out_relres = c->w_relres;
     d.out_status = c->w_status;

@@ -388,6 +388,49 @@ def hmc_compare(T, d, rank, ntraj, theta=None, lattice=None, seed=1234, maxiter=
     return res
 
 
+def analysis_batches(T, local, nconf=8):
+    """The batched analyzer on the finite-volume scan's extremes (Nt = 64,
+    Nx = 32 and 96, Ls = 16, m_f = 0.05, seeded beta = 3 configurations):
+    nconf configurations per call, each with 2 spins x 4 point-source times,
+    16 boundary Z4 noise sources and 2 spins x 2 wall-source times (28
+    right-hand sides), solved together by the even-odd mixed solver to 1e-10
+    and contracted (C_PP, C_J5, loop, momentum C_PP). Device time of the call
+    (CUDA events on the library stream, host copies of configurations and
+    correlators included) per configuration and per right-hand side."""
+    import torch
+    from three_part_dwf_study_b200.ensemble import quenched_theta
+    from three_part_dwf_study_b200.rng import z4_digits
+    out = {}
+    for Nx in (32, 96):
+        Nt, Ls = 64, 16
+        d = T.DomainWall(Nt, Nx, Ls, M5, MF, BETA, device=local)
+        st = torch.cuda.ExternalStream(d.stream_ptr())
+        rng = np.random.default_rng(GAUGE_SEED + Nx)
+        th = np.stack([quenched_theta(rng, Nt, Nx, BETA) for _ in range(nconf)])
+        z4 = np.concatenate([z4_digits(NOISE_SEED + 104729 * k, N_NOISE * Nt * Nx * 2)
+                             for k in range(nconf)])
+        kw = dict(z4=z4, n_point_times=4, n_wall_times=2, n_noise=N_NOISE, max_momentum=5,
+                  rtol=RTOL, maxiter=MAXITER, solver=T.SOLVER_EO_MIXED)
+        d.measure(th, **kw)  # warm-up (autotuning, allocations)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        m = d.measure(th, **kw)
+        e1.record(st)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3
+        if not all(i["converged"] for i in m["info"]):
+            raise SystemExit(f"analysis batch did not converge (Nx={Nx})")
+        nr = len(m["info"])
+        out[f"64x{Nx}x16"] = {"configurations": nconf, "rhs": nr,
+                              "seconds_per_configuration": sec / nconf,
+                              "solves_per_s": nr / sec,
+                              "schur_iterations_mean": statistics.mean(i["schur_iterations"] for i in m["info"])}
+        d.close()
+    return out
+
+
 # DWF 128x128, Ls = 24, M5 = 1, m_f = 0.02, beta = 4: the larger HMC comparison
 C5_LATTICE, C5_M5, C5_MF, C5_BETA = (128, 128, 24), 1.0, 0.02, 4.0
 
@@ -656,6 +699,7 @@ def impl_ours(args):
     # ---- HMC on the same lattice: FP64 and mixed CG on the same trajectories ----
     hmc = hmc_compare(T, d, rank, args.hmc_trajectories)
     hmc_large = hmc_compare_large(T, local, args.hmc_large_trajectories) if ws == 1 else None
+    analysis = analysis_batches(T, local) if (args.analysis and ws == 1) else None
     # ---- Wilson 64x64 near the critical mass with the learned preconditioner ----
     wil = wilson_learned_grid(T) if (args.wilson_learned and ws == 1) else None
 
@@ -739,6 +783,7 @@ def impl_ours(args):
         "dslash": dslash,
         "hmc": hmc,
         "hmc_128x128x24": hmc_large,
+        "analysis_batched": analysis,
         "learned_wilson_64x64": wil,
         "gpu_launches": launches,
         "clocks": clocks,
@@ -913,6 +958,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
+    ap.add_argument("--no-analysis", dest="analysis", action="store_false",
+                    help="skip the batched-analyzer timing (Nt=64, Nx=32 and 96)")
     ap.add_argument("--hmc-large-trajectories", type=int, default=1,
                     help="HMC trajectories of the 128x128x24 FP64-vs-mixed comparison (0: skip)")
     ap.add_argument("--hmc-trajectories", type=int, default=2,

@@ -439,7 +439,7 @@ int dwf_lp_time_network(dwf_ctx* ctx, int nrhs, int reps, double* ms_per_apply, 
  * not fit). */
 int dwf_lp_set_variant(dwf_ctx* ctx, int variant);
 /* Inner solve: stop at |r| <= inner_tol |r0| or inner_maxiter iterations;
- * at most outer_max defect-correction cycles (defaults 1e-4, 400, 40). */
+ * at most outer_max defect-correction cycles (defaults 3e-4, 400, 40). */
 int dwf_lp_set_solver(dwf_ctx* ctx, double inner_tol, int inner_maxiter, int outer_max);
 
 

@@ -129,6 +129,6 @@ class LearnedMixin:
         times both kernels and keeps the faster), 0 mma.sync, 1 tcgen05."""
         self._check(A.lib().dwf_lp_set_variant(self._h, int(variant)))
 
-    def lp_set_solver(self, inner_tol=1e-4, inner_maxiter=400, outer_max=40):
+    def lp_set_solver(self, inner_tol=3e-4, inner_maxiter=400, outer_max=40):
         self._check(A.lib().dwf_lp_set_solver(self._h, float(inner_tol), int(inner_maxiter),
                                               int(outer_max)))

@@ -373,20 +373,23 @@ __global__ void __launch_bounds__(kConvWarps * 32) lp_conv_kernel(ConvArgs a)
 // ---------------------------------------------------------------------------
 // PTC layer on the 5th-generation tensor cores (tcgen05, accumulators in TMEM)
 // ---------------------------------------------------------------------------
-// A CTA of 4 warps owns a tile of 128 consecutive lattice sites (lexicographic
-// h = t Nx + x) of one right-hand side. The input around the tile (sites
-// h0 - Nx .. h0 + 127 + Nx) is staged in shared memory as BF16 in three
-// copies, copy dx holding in(t, x + dx) at the position of (t, x), so that
-// the operand of every offset (dt, dx) is a contiguous 128-row window of one
-// copy, (1 + dt) Nx rows from its start. Layout of a copy: planes of 4
-// complex channels (16 B per site), the canonical no-swizzle K-major layout
-// of tcgen05.mma (rows 16 B apart, 8-row groups 128 B apart, the two 16-B
-// K-chunks of a k-step one plane apart). The weights are the B operand
-// (N = 2 cout real columns, K-major). One elected thread issues, per offset,
-// cpad/8 MMAs of 128 x N x 16 into one of two TMEM accumulators and commits
-// them to an mbarrier; meanwhile the 4 warps read the other accumulator
-// (tcgen05.ld, one row per thread), multiply by that row's FP32 transporter
-// and add into FP32 registers.
+// Sites are addressed in padded rows: lattice row t holds P = Nx + 2 rows,
+// row t P + 1 + x for site (t, x) and one halo row on each side (x = -1 and
+// x = Nx, i.e. the wrapped neighbours). A CTA owns tiles of 128 consecutive
+// padded rows of one right-hand side; the input around a tile (padded rows
+// pr0 - P - 1 .. pr0 + 127 + P + 1) is staged once in shared memory as BF16,
+// double-buffered across tiles, so that the operand of every offset
+// (dt, dx) is the contiguous 128-row window starting (1 + dt) P + 1 + dx rows
+// into the staged window (a row shift of the MMA's start address). Layout of
+// the window: planes of 4 complex channels (16 B per row), the canonical
+// no-swizzle K-major layout of tcgen05.mma (rows 16 B apart, 8-row groups
+// 128 B apart, the two 16-B K-chunks of a k-step one plane apart). The
+// weights are the B operand (N = 2 cout real columns, K-major). One elected
+// thread issues, per offset, cpad/8 MMAs of 128 x N x 16 into one of four
+// TMEM accumulators and commits them to an mbarrier; meanwhile the 4
+// epilogue warps read a finished accumulator (tcgen05.ld, one row per
+// thread), multiply by that row's FP32 transporter and add into FP32
+// registers. Halo rows are computed and dropped.
 struct TcArgs
 {
     const float2* in;
@@ -409,10 +412,20 @@ struct TcArgs
 
 constexpr int kTcM = 128;
 
+// Staged window of one tile in padded rows: lattice rows stored with one
+// halo site on each side (P = Nx + 2 rows per lattice row), the tile's 128
+// rows plus one padded lattice row and one site on each side.
+__host__ __device__ __forceinline__ int tc_window_rows(int Nx) { return kTcM + 2 * (Nx + 2) + 2; }
+
 __host__ __device__ __forceinline__ size_t tc_smem_bytes(int cpad, int ncol, int Nx)
 {
-    const size_t J = size_t(kTcM) + 2 * size_t(Nx);
-    return size_t(9) * (cpad / 8) * 2 * ncol * 16 + size_t(3) * (cpad / 4) * J * 16;
+    return size_t(9) * (cpad / 8) * 2 * ncol * 16 + size_t(2) * (cpad / 4) * tc_window_rows(Nx) * 16;
+}
+
+// Tiles of 128 padded rows per right-hand side.
+__host__ __device__ __forceinline__ long tc_tiles_per_rhs(int Nt, int Nx)
+{
+    return (long(Nt) * (Nx + 2) + kTcM - 1) / kTcM;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -574,54 +587,13 @@ __device__ __forceinline__ bool mbar_wait_lean(uint32_t mbar, uint32_t parity, u
     }
 }
 
-// Stage the three x-shifted BF16 copies of the tile's input window.
-template <bool kPlanar>
-__device__ __forceinline__ void tc_stage(const TcArgs& a, uint4* As, int J, int planes, int h0, int rhs)
-{
-    const int nthr = blockDim.x;
-    for (int j = threadIdx.x; j < J; j += nthr)
-    {
-        int hs = h0 - a.Nx + j;
-        hs = hs < 0 ? hs + a.V : (hs >= a.V ? hs - a.V : hs);
-        hs = hs >= a.V ? hs % a.V : hs;  // tiles shorter than a row pair on tiny lattices
-        const int t = hs / a.Nx, x = hs - t * a.Nx;
-        const int row = t * a.Nx;
-        const int xm = (x == 0) ? a.Nx - 1 : x - 1;
-        const int xp = (x == a.Nx - 1) ? 0 : x + 1;
-        const int src[3] = {row + xm, row + x, row + xp};
-#pragma unroll
-        for (int dxi = 0; dxi < 3; ++dxi)
-        {
-            if (kPlanar)
-            {
-                const uint4* base = a.in_bf + long(rhs) * planes * a.V + src[dxi];
-                for (int pl = 0; pl < planes; ++pl)
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                                     smem_u32(As + (dxi * planes + pl) * J + j)),
-                                 "l"(base + long(pl) * a.V)
-                                 : "memory");
-            }
-            else
-            {
-                const float2* inr = a.in + long(rhs) * a.li.rs;
-                for (int pl = 0; pl < planes; ++pl)
-                    As[(dxi * planes + pl) * J + j] = load_plane(inr, a.li, a.cin, src[dxi], 4 * pl);
-            }
-        }
-    }
-}
-
-// Offsets in the order the MMAs consume them: dx = -1 (copy 0), dx = 0
-// (copy 1), dx = +1 (copy 2), so that each copy is released for the next tile
-// after its third offset.
-__constant__ int kTcOrder[9] = {4, 6, 8, 0, 1, 2, 3, 5, 7};
-
 // Warp roles of the tcgen05 layer kernel (kTcThreads = 256):
-//   warps 0-3  epilogue: one TMEM lane (output site) per thread, all columns
+//   warps 0-3  epilogue: one TMEM lane (output row) per thread, all columns
 //   warp 4     MMA issue (one elected thread)
-//   warps 5-7  producers: stage copy c of the next tile into shared memory as
-//              soon as the MMAs of the current tile are done with it
-// mbarriers: tfull[s] / tempty[s] per TMEM slot, cfull[c] / cfree[c] per copy.
+//   warps 5-7  producers: stage the window of tile n into buffer n % 2 as
+//              soon as the MMAs of tile n - 2 are done with it
+// mbarriers: tfull[s] / tempty[s] per TMEM slot, wfull[b] / wfree[b] per
+// window buffer.
 constexpr int kEpiWarps = 4;
 constexpr int kProdWarps = 3;
 
@@ -640,15 +612,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
     const int ksp = a.cpad / 8;
     const int nks = 9 * ksp;
     const int planes = a.cpad / 4;
-    const int J = kTcM + 2 * a.Nx;
+    const int P = a.Nx + 2;                 // padded rows per lattice row
+    const int J = tc_window_rows(a.Nx);     // staged rows per tile
+    const long NP = long(a.Nt) * P;         // padded rows per right-hand side
     uint4* Bs = reinterpret_cast<uint4*>(smem);
-    uint4* As = Bs + nks * 2 * NCOL;
+    uint4* As = Bs + nks * 2 * NCOL;        // [buffer][plane][row]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t mb = smem_u32(&mbar[0]);
     auto TFULL = [&](int sl) { return mb + 8u * uint32_t(sl); };
     auto TEMPTY = [&](int sl) { return mb + 8u * uint32_t(kSlots + sl); };
-    auto CFULL = [&](int c) { return mb + 8u * uint32_t(2 * kSlots + c); };
-    auto CFREE = [&](int c) { return mb + 8u * uint32_t(2 * kSlots + 3 + c); };
+    auto WFULL = [&](int b) { return mb + 8u * uint32_t(2 * kSlots + b); };
+    auto WFREE = [&](int b) { return mb + 8u * uint32_t(2 * kSlots + 2 + b); };
     for (int i = tid; i < nks * 2 * NCOL; i += blockDim.x)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(Bs + i)), "l"(a.B + i) : "memory");
     asm volatile("cp.async.wait_all;" ::: "memory");
@@ -659,10 +633,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(TFULL(i)), "r"(1u));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(TEMPTY(i)), "r"(uint32_t(kEpiWarps)));
         }
-        for (int c = 0; c < 3; ++c)
+        for (int b = 0; b < 2; ++b)
         {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(CFULL(c)), "r"(uint32_t(kProdWarps * 32)));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(CFREE(c)), "r"(1u));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(WFULL(b)), "r"(uint32_t(kProdWarps * 32)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(WFREE(b)), "r"(1u));
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -677,7 +651,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_holder;
-    const long tiles_per_rhs = (a.V + kTcM - 1) / kTcM;
+    const long tiles_per_rhs = tc_tiles_per_rhs(a.Nt, a.Nx);
     const long ntiles = tiles_per_rhs * a.nrhs;
     bool ok = true;
 
@@ -686,57 +660,54 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
         // ---- producers ----
         const int pt = tid - (kEpiWarps + 1) * 32;  // 0 .. 95
         const int nprod = kProdWarps * 32;
-        uint32_t free_ph = 0u;  // bit c: next cfree phase
+        uint32_t free_ph = 0u;  // bit b: next wfree phase
         long it = 0;
         for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++it)
         {
             const int rhs = int(tl / tiles_per_rhs);
-            const int h0 = int(tl - long(rhs) * tiles_per_rhs) * kTcM;
-            for (int c = 0; c < 3; ++c)
+            const long pr0 = (tl - long(rhs) * tiles_per_rhs) * kTcM;
+            const int bf = int(it & 1);
+            if (it >= 2)
             {
-                if (it > 0)
-                {
-                    // the MMAs of the previous tile are done with copy c
-                    if (!mbar_wait_lean(CFREE(c), (free_ph >> c) & 1u, a.timeout_ns))
-                        ok = false;
-                    free_ph ^= 1u << c;
-                }
-                const int dx = c - 1;
-                for (int j = pt; j < J; j += nprod)
-                {
-                    int hs = h0 - a.Nx + j;
-                    hs = hs < 0 ? hs + a.V : (hs >= a.V ? hs - a.V : hs);
-                    hs = hs >= a.V ? hs % a.V : hs;
-                    const int t = hs / a.Nx, x = hs - t * a.Nx;
-                    int x2 = x + dx;
-                    x2 = x2 < 0 ? x2 + a.Nx : (x2 >= a.Nx ? x2 - a.Nx : x2);
-                    const int src = t * a.Nx + x2;
-                    if (a.in_bf)
-                    {
-                        const uint4* base = a.in_bf + long(rhs) * planes * a.V + src;
-                        for (int pl = 0; pl < planes; ++pl)
-                            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                                             smem_u32(As + (c * planes + pl) * J + j)),
-                                         "l"(base + long(pl) * a.V)
-                                         : "memory");
-                    }
-                    else
-                    {
-                        const float2* inr = a.in + long(rhs) * a.li.rs;
-                        for (int pl = 0; pl < planes; ++pl)
-                            As[(c * planes + pl) * J + j] = load_plane(inr, a.li, a.cin, src, 4 * pl);
-                    }
-                }
+                // the MMAs of tile it - 2 are done with this buffer
+                if (!mbar_wait_lean(WFREE(bf), (free_ph >> bf) & 1u, a.timeout_ns))
+                    ok = false;
+                free_ph ^= 1u << bf;
+            }
+            uint4* Ab = As + long(bf) * planes * J;
+            for (int j = pt; j < J; j += nprod)
+            {
+                // padded row pr0 - P - 1 + j, wrapped over the lattice's rows
+                long pr = (pr0 - P - 1 + j) % NP;
+                pr = pr < 0 ? pr + NP : pr;
+                const int t = int(pr / P), xp = int(pr - long(t) * P);
+                const int x = (xp == 0) ? a.Nx - 1 : ((xp == P - 1) ? 0 : xp - 1);
+                const int src = t * a.Nx + x;
                 if (a.in_bf)
                 {
-                    // arrives once this thread's copies have landed
-                    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(CFULL(c)) : "memory");
+                    const uint4* base = a.in_bf + long(rhs) * planes * a.V + src;
+                    for (int pl = 0; pl < planes; ++pl)
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                         smem_u32(Ab + pl * J + j)),
+                                     "l"(base + long(pl) * a.V)
+                                     : "memory");
                 }
                 else
                 {
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    mbar_arrive(CFULL(c));
+                    const float2* inr = a.in + long(rhs) * a.li.rs;
+                    for (int pl = 0; pl < planes; ++pl)
+                        Ab[pl * J + j] = load_plane(inr, a.li, a.cin, src, 4 * pl);
                 }
+            }
+            if (a.in_bf)
+            {
+                // arrives once this thread's copies have landed
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(WFULL(bf)) : "memory");
+            }
+            else
+            {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(WFULL(bf));
             }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
@@ -751,23 +722,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
             const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
             const uint32_t a_lbo = uint32_t(J) * 16u;
             const uint32_t b_lbo = uint32_t(NCOL) * 16u;
-            uint32_t full_ph = 0u;   // bit c: next cfull phase
+            uint32_t full_ph = 0u;   // bit b: next wfull phase
             uint32_t empty_ph = 0u;  // bit s: next tempty phase
             uint32_t used = 0u;
             uint32_t g = 0;          // offsets issued so far
-            for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x)
+            long it = 0;
+            for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++it)
             {
-                for (int q = 0; q < 9; ++q, ++g)
+                const int bf = int(it & 1);
+                if (!mbar_wait_lean(WFULL(bf), (full_ph >> bf) & 1u, a.timeout_ns))
+                    ok = false;
+                full_ph ^= 1u << bf;
+                // the producers' copies become visible to the tensor cores
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const uint32_t wbase = a_base + uint32_t(bf * planes * J) * 16u;
+                for (int k = 0; k < 9; ++k, ++g)
                 {
-                    const int c = q / 3;
-                    if (q % 3 == 0)
-                    {
-                        if (!mbar_wait_lean(CFULL(c), (full_ph >> c) & 1u, a.timeout_ns))
-                            ok = false;
-                        full_ph ^= 1u << c;
-                        // the producers' copies become visible to the tensor cores
-                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    }
                     const int sl = int(g % kSlots);
                     if (used & (1u << sl))
                     {
@@ -777,27 +747,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
                     }
                     used |= 1u << sl;
                     tc_fence_after();
-                    const int k = kTcOrder[q];
-                    const int dt = kOffT[k];
+                    // window row of output row 0 for this offset
+                    const int row0 = (1 + kOffT[k]) * P + 1 + kOffX[k];
                     const uint32_t d_tmem = tmem + uint32_t(sl) * uint32_t(NCOL);
                     for (int ks = 0; ks < ksp; ++ks)
                     {
-                        const uint32_t aaddr = a_base + uint32_t((c * planes + 2 * ks) * J + (1 + dt) * a.Nx) * 16u;
+                        const uint32_t aaddr = wbase + uint32_t((2 * ks) * J + row0) * 16u;
                         const uint32_t baddr = b_base + uint32_t((k * ksp + ks) * 2 * NCOL) * 16u;
                         tc_mma(d_tmem, umma_desc(aaddr, a_lbo, 128u), umma_desc(baddr, b_lbo, 128u), idesc,
                                ks > 0 ? 1u : 0u);
                     }
                     tc_commit(TFULL(sl));
-                    if (q % 3 == 2)
-                        tc_commit(CFREE(c));
                 }
+                tc_commit(WFREE(bf));
             }
-            // the copy-release arrivals of the last tile land before the CTA exits
+            // the buffer-release arrivals of the last tiles land before the CTA exits
             const long mine = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
-            if (mine > 0)
-                for (int c = 0; c < 3; ++c)
-                    if (!mbar_wait_lean(CFREE(c), uint32_t((mine - 1) & 1), a.timeout_ns))
-                        ok = false;
+            for (int bf = 0; bf < 2; ++bf)
+            {
+                const long uses = (mine + 1 - bf) / 2;   // tiles that used buffer bf
+                if (uses > 0 && !mbar_wait_lean(WFREE(bf), uint32_t((uses - 1) & 1), a.timeout_ns))
+                    ok = false;
+            }
         }
         __syncwarp();
     }
@@ -810,10 +781,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
         for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x)
         {
             const int rhs = int(tl / tiles_per_rhs);
-            const int h0 = int(tl - long(rhs) * tiles_per_rhs) * kTcM;
+            const long pr = (tl - long(rhs) * tiles_per_rhs) * kTcM + erow;   // this thread's padded row
             const int cf = a.conf ? a.conf[rhs] : a.conf0;
-            const int hrow = h0 + erow;
-            const bool row_ok = hrow < a.V;
+            const int tr = int(pr / P), xp = int(pr - long(tr) * P);
+            // halo rows (xp = 0, P - 1) and rows past the lattice are dropped
+            const bool row_ok = pr < NP && xp >= 1 && xp <= a.Nx;
+            const int hrow = row_ok ? tr * a.Nx + xp - 1 : 0;
             float2 Tk[9];
             {
                 const float2* Tc = a.T + (long(cf) * a.V + (row_ok ? hrow : 0)) * 9;
@@ -833,7 +806,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
                     ok = false;
                 full_ph ^= 1u << sl;
                 tc_fence_after();
-                const int k = kTcOrder[q];
+                const int k = q;   // the MMAs run the offsets in order
                 float2 T = Tk[0];
 #pragma unroll
                 for (int u = 1; u < 9; ++u)
@@ -1830,7 +1803,7 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
         t.timeout_ns = c->timeout_ns;
         t.in_bf = in_bf;
         t.out_bf = out_bf;
-        const long ntiles = long((c->L.V + kTcM - 1) / kTcM) * nrhs;
+        const long ntiles = tc_tiles_per_rhs(c->L.Nt, c->L.Nx) * nrhs;
         const int grid = int(std::max<long>(1, std::min<long>(ntiles, long(c->nsm))));
         ST(set_conv_smem(c));
         switch (ncol)

@@ -408,6 +408,7 @@ struct TcArgs
     // the output written to out_bf instead of `out`
     const uint4* in_bf;
     uint4* out_bf;
+    int nbuf;   // window buffers per CTA (1: two CTAs share an SM; 2: one CTA, double-buffered)
 };
 
 constexpr int kTcM = 128;
@@ -417,9 +418,15 @@ constexpr int kTcM = 128;
 // rows plus one padded lattice row and one site on each side.
 __host__ __device__ __forceinline__ int tc_window_rows(int Nx) { return kTcM + 2 * (Nx + 2) + 2; }
 
-__host__ __device__ __forceinline__ size_t tc_smem_bytes(int cpad, int ncol, int Nx)
+__host__ __device__ __forceinline__ size_t tc_smem_bytes(int cpad, int ncol, int Nx, int nbuf)
 {
-    return size_t(9) * (cpad / 8) * 2 * ncol * 16 + size_t(2) * (cpad / 4) * tc_window_rows(Nx) * 16;
+    return size_t(9) * (cpad / 8) * 2 * ncol * 16 + size_t(nbuf) * (cpad / 4) * tc_window_rows(Nx) * 16;
+}
+
+// TMEM columns one CTA allocates (kSlots accumulators of ncol columns, a power of 2 >= 64).
+__host__ __device__ constexpr uint32_t tc_tmem_cols(int ncol)
+{
+    return (4 * ncol <= 64) ? 64u : (4 * ncol <= 128) ? 128u : (4 * ncol <= 256) ? 256u : 512u;
 }
 
 // Tiles of 128 padded rows per right-hand side.
@@ -590,24 +597,23 @@ __device__ __forceinline__ bool mbar_wait_lean(uint32_t mbar, uint32_t parity, u
 // Warp roles of the tcgen05 layer kernel (kTcThreads = 256):
 //   warps 0-3  epilogue: one TMEM lane (output row) per thread, all columns
 //   warp 4     MMA issue (one elected thread)
-//   warps 5-7  producers: stage the window of tile n into buffer n % 2 as
-//              soon as the MMAs of tile n - 2 are done with it
+//   warps 5-7  producers: stage the window of tile n into buffer n % nbuf as
+//              soon as the MMAs of tile n - nbuf are done with it
 // mbarriers: tfull[s] / tempty[s] per TMEM slot, wfull[b] / wfree[b] per
 // window buffer.
 constexpr int kEpiWarps = 4;
 constexpr int kProdWarps = 3;
 
 template <int NCOL>
-__global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
+__global__ void __launch_bounds__(kTcThreads, 2) lp_tc_kernel(TcArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int kSlots = 4;
     __shared__ __align__(8) uint64_t mbar[2 * kSlots + 6];
     __shared__ uint32_t tmem_holder;
     constexpr int NC = NCOL / 2;
-    constexpr uint32_t kCols = (kSlots * NCOL <= 64) ? 64u
-                               : (kSlots * NCOL <= 128) ? 128u
-                               : (kSlots * NCOL <= 256) ? 256u : 512u;
+    static_assert(kSlots == 4, "tc_tmem_cols assumes four accumulator slots");
+    constexpr uint32_t kCols = tc_tmem_cols(NCOL);
     static_assert(NC >= 1 && kSlots * NCOL <= 512, "TMEM columns");
     const int ksp = a.cpad / 8;
     const int nks = 9 * ksp;
@@ -666,10 +672,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
         {
             const int rhs = int(tl / tiles_per_rhs);
             const long pr0 = (tl - long(rhs) * tiles_per_rhs) * kTcM;
-            const int bf = int(it & 1);
-            if (it >= 2)
+            const int bf = int(it % a.nbuf);
+            if (it >= a.nbuf)
             {
-                // the MMAs of tile it - 2 are done with this buffer
+                // the MMAs of tile it - nbuf are done with this buffer
                 if (!mbar_wait_lean(WFREE(bf), (free_ph >> bf) & 1u, a.timeout_ns))
                     ok = false;
                 free_ph ^= 1u << bf;
@@ -729,7 +735,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
             long it = 0;
             for (long tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++it)
             {
-                const int bf = int(it & 1);
+                const int bf = int(it % a.nbuf);
                 if (!mbar_wait_lean(WFULL(bf), (full_ph >> bf) & 1u, a.timeout_ns))
                     ok = false;
                 full_ph ^= 1u << bf;
@@ -763,9 +769,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) lp_tc_kernel(TcArgs a)
             }
             // the buffer-release arrivals of the last tiles land before the CTA exits
             const long mine = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
-            for (int bf = 0; bf < 2; ++bf)
+            for (int bf = 0; bf < a.nbuf; ++bf)
             {
-                const long uses = (mine + 1 - bf) / 2;   // tiles that used buffer bf
+                const long uses = (mine + a.nbuf - 1 - bf) / a.nbuf;   // tiles that used buffer bf
                 if (uses > 0 && !mbar_wait_lean(WFREE(bf), uint32_t((uses - 1) & 1), a.timeout_ns))
                     ok = false;
             }
@@ -1765,7 +1771,7 @@ bool tc_fits(const dwf_ctx* c, int l, bool adjoint)
     const int ci = adjoint ? n->cout[l] : n->cin[l];
     const int co = adjoint ? n->cin[l] : n->cout[l];
     const int ncol = ncol_of(co);
-    return ncol <= 96 && tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx) <= size_t(220 * 1024);
+    return ncol <= 96 && tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx, 1) <= size_t(220 * 1024);
 }
 
 // One layer (forward or adjoint) on device fields. in_bf / out_bf (tcgen05
@@ -1778,7 +1784,12 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
     const int ci = adjoint ? n->cout[l] : n->cin[l];
     const int co = adjoint ? n->cin[l] : n->cout[l];
     const int ncol = ncol_of(co);
-    const size_t tsm = tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx);
+    // two CTAs per SM (one window buffer each) where their shared memory and
+    // TMEM fit, else one double-buffered CTA
+    const bool two = 2 * tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx, 1) <= size_t(226 * 1024) &&
+                     2 * tc_tmem_cols(ncol) <= 512u;
+    const int nbuf = two ? 1 : 2;
+    const size_t tsm = tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx, nbuf);
     const bool tc_ok = tc_fits(c, l, adjoint);
     if (lp_tc_allowed(n) && tc_ok)
     {
@@ -1803,8 +1814,9 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
         t.timeout_ns = c->timeout_ns;
         t.in_bf = in_bf;
         t.out_bf = out_bf;
+        t.nbuf = nbuf;
         const long ntiles = tc_tiles_per_rhs(c->L.Nt, c->L.Nx) * nrhs;
-        const int grid = int(std::max<long>(1, std::min<long>(ntiles, long(c->nsm))));
+        const int grid = int(std::max<long>(1, std::min<long>(ntiles, long(two ? 2 : 1) * c->nsm)));
         ST(set_conv_smem(c));
         switch (ncol)
         {

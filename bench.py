@@ -884,6 +884,21 @@ def profile_dslash():
     return 0
 
 
+def profile_network():
+    """Network applications only (for ncu captures of the layer kernel): the
+    bench's 32-channel network with its initial weights on the workload
+    configuration, applied to 28 Gaussian fields 6 times."""
+    import three_part_dwf_study_b200 as T
+    d = T.DomainWall(NT, NX, LS, M5, MF, BETA)
+    d.set_gauge(workload_gauge(0))
+    d.lp_init(hidden=LP_HIDDEN, seed=5)
+    d.lp_set_variant(1)
+    ms, _ = d.lp_time_network(28, 5)
+    print(json.dumps({"network_ms_per_application": ms}))
+    d.close()
+    return 0
+
+
 def eo_phases():
     """Per-phase device time of the even-odd solver kernel on one propagator
     batch of the workload (one JSON line, us per iteration)."""
@@ -969,6 +984,7 @@ def main():
     ap.add_argument("--profile-case", action="store_true")
     ap.add_argument("--profile-dslash", action="store_true")
     ap.add_argument("--profile-learned", action="store_true")
+    ap.add_argument("--profile-network", action="store_true")
     ap.add_argument("--dslash-variants", action="store_true")
     ap.add_argument("--eo-phases", action="store_true")
     args = ap.parse_args()
@@ -978,6 +994,8 @@ def main():
         return profile_dslash()
     if args.profile_learned:
         return profile_learned()
+    if args.profile_network:
+        return profile_network()
     if args.dslash_variants:
         return dslash_variants()
     if args.eo_phases:

@@ -129,13 +129,16 @@ def test_loss_and_gradient_match_oracle(T, torch, variant):
     d.close()
 
 
-def test_layer_variants_agree_at_width_32(T, torch):
-    """tcgen05 and mma.sync layers on a 32-channel domain-wall field (Ls = 16,
-    hidden 32: the widths of the benchmark) agree to FP32 accumulation order."""
-    rng = np.random.default_rng(17)
-    d = T.DomainWall(16, 64, 16, 1.0, 0.05)
+@pytest.mark.parametrize("Ls,hidden", [(16, 32), (12, 24), (24, 16), (20, 24)])
+def test_layer_variants_agree_at_wide_layers(T, torch, Ls, hidden):
+    """tcgen05 and mma.sync networks on wide domain-wall fields agree to FP32
+    accumulation order: the benchmark's widths (Ls = 16, hidden 32: 64 real
+    columns, two CTAs per SM), 24 channels (48 columns, 8-column TMEM loads),
+    48 channels (96 columns, one double-buffered CTA) and 40 channels."""
+    rng = np.random.default_rng(17 + Ls + hidden)
+    d = T.DomainWall(16, 64, Ls, 1.0, 0.05)
     d.set_gauge(quenched_theta(rng, 16, 64, 3.0)[None])
-    d.lp_init(hidden=32, seed=2)
+    d.lp_init(hidden=hidden, seed=2)
     f = torch.from_numpy(crand(rng, 3, d.Ndof)).cuda()
     outs = []
     for v in (1, 0):

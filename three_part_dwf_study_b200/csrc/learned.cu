@@ -1650,9 +1650,20 @@ int lp_grow(dwf_ctx* c, T*& p, size_t n)
     return DWF_OK;
 }
 
-int nt_of(int cout) { return (2 * cout + 7) / 8; }
+// Output column tiles of the mma.sync layer (8 real columns each) and real
+// output columns of the tcgen05 layer, rounded up to the instantiated kernel
+// shapes (the padded columns hold zero weights and are not stored).
+int nt_of(int cout)
+{
+    const int n = (2 * cout + 7) / 8;
+    return n <= 2 ? n : (n <= 4 ? 4 : (n <= 6 ? 6 : (n <= 8 ? 8 : 12)));
+}
 
-int ncol_of(int cout) { return (2 * cout + 15) / 16 * 16; }
+int ncol_of(int cout)
+{
+    const int n = (2 * cout + 15) / 16 * 16;
+    return n <= 64 ? n : 96;
+}
 
 int grid_for(long n, int nsm) { return int(std::max<long>(1, std::min<long>((n + 255) / 256, 8L * nsm))); }
 

@@ -129,15 +129,18 @@ def test_loss_and_gradient_match_oracle(T, torch, variant):
     d.close()
 
 
-@pytest.mark.parametrize("Ls,hidden", [(16, 32), (12, 24), (24, 16), (20, 24)])
-def test_layer_variants_agree_at_wide_layers(T, torch, Ls, hidden):
+@pytest.mark.parametrize("Ls,hidden,Nt,Nx", [(16, 32, 16, 64), (12, 24, 16, 64), (24, 16, 16, 64),
+                                          (20, 24, 16, 64), (16, 32, 4, 256)])
+def test_layer_variants_agree_at_wide_layers(T, torch, Ls, hidden, Nt, Nx):
     """tcgen05 and mma.sync networks on wide domain-wall fields agree to FP32
     accumulation order: the benchmark's widths (Ls = 16, hidden 32: 64 real
     columns, two CTAs per SM), 24 channels (48 columns, 8-column TMEM loads),
-    48 channels (96 columns, one double-buffered CTA) and 40 channels."""
-    rng = np.random.default_rng(17 + Ls + hidden)
-    d = T.DomainWall(16, 64, Ls, 1.0, 0.05)
-    d.set_gauge(quenched_theta(rng, 16, 64, 3.0)[None])
+    48 channels (96 columns, one double-buffered CTA), 40 channels, and 32
+    channels at Nx = 256 (one CTA per SM with a single window buffer: two
+    buffers would exceed the shared memory)."""
+    rng = np.random.default_rng(17 + Ls + hidden + Nx)
+    d = T.DomainWall(Nt, Nx, Ls, 1.0, 0.05)
+    d.set_gauge(quenched_theta(rng, Nt, Nx, 3.0)[None])
     d.lp_init(hidden=hidden, seed=2)
     f = torch.from_numpy(crand(rng, 3, d.Ndof)).cuda()
     outs = []

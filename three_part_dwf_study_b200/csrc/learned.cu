@@ -1799,7 +1799,8 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
     // TMEM fit, else one double-buffered CTA
     const bool two = 2 * tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx, 1) <= size_t(226 * 1024) &&
                      2 * tc_tmem_cols(ncol) <= 512u;
-    const int nbuf = two ? 1 : 2;
+    // one CTA double-buffers its window where the second buffer still fits
+    const int nbuf = (two || tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx, 2) > size_t(220 * 1024)) ? 1 : 2;
     const size_t tsm = tc_smem_bytes(cpad_of(ci), ncol, c->L.Nx, nbuf);
     const bool tc_ok = tc_fits(c, l, adjoint);
     if (lp_tc_allowed(n) && tc_ok)

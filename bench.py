@@ -504,6 +504,41 @@ def wilson_learned_grid(T, ntrain=8):
     return out
 
 
+WILSON_DSLASH_LATTICE = (2048, 2048)
+
+
+def wilson_dslash(T, local, dev, peak):
+    """Standalone Wilson D at 2048x2048 (working set ~400 MB >> L2) in complex128
+    and complex64: V*(2*4w + 2*2w) bytes per application (spinor in and out,
+    two complex links), 96 B (FP64) / 48 B (FP32) per site; the autotuned
+    kernel, 20 back-to-back applications timed with CUDA events."""
+    import torch
+    Nt, Nx = WILSON_DSLASH_LATTICE
+    w = T.Wilson(Nt, Nx, 0.1, 0.0, device=local)
+    w.set_gauge(np.random.default_rng(4).uniform(-np.pi, np.pi, 2 * Nt * Nx))
+    st = torch.cuda.ExternalStream(w.stream_ptr(), device=dev)
+    out = {"lattice": [Nt, Nx], "bytes_rule": "V*96 B (FP64), V*48 B (FP32) per application"}
+    for prec, dt, wb in ((64, torch.float64, 8), (32, torch.float32, 4)):
+        a = torch.randn(w.Ndof * 2, dtype=dt, device=dev)
+        b = torch.empty_like(a)
+        for _ in range(3):
+            w.apply_dev(0, a, b)
+        w.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(20):
+            w.apply_dev(0, a, b)
+        e1.record(st)
+        e1.synchronize()
+        tsec = e0.elapsed_time(e1) * 1e-3 / 20
+        gbs = Nt * Nx * (2 * 4 * wb + 2 * 2 * wb) / tsec / 1e9
+        out[f"complex{2 * prec}"] = {"GBs": round(gbs, 1), "frac": round(gbs / peak, 4),
+                                     "us_per_apply": round(tsec * 1e6, 2)}
+    w.close()
+    return out
+
+
 def workload_config(solver):
     return {
         "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, seeded beta=3.0 "
@@ -695,6 +730,8 @@ def impl_ours(args):
                                          "us_per_apply": round(tsec * 1e6, 2)}
     dslash["lattice"] = list(DSLASH_LATTICE)
     dslash["bytes_rule"] = "V*(Ls*64+32) B (FP64), V*(Ls*32+16) B (FP32) per application"
+    dd.close()
+    dslash["wilson"] = wilson_dslash(T, local, dev, peak)
 
     # ---- HMC on the same lattice: FP64 and mixed CG on the same trajectories ----
     hmc = hmc_compare(T, d, rank, args.hmc_trajectories)

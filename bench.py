@@ -965,24 +965,32 @@ def eo_phases():
 
 def dslash_variants():
     """Event-timed GB/s of the Dslash kernels (site, column, site with shuffled
-    x neighbours, t sweep at the automatic and at fixed chunk lengths) in FP64
-    and FP32 at 256x256x16 and 512x512x16 (one JSON line)."""
+    x neighbours, t sweep at the automatic and at fixed chunk lengths, and for
+    Wilson the row kernel) in FP64
+    and FP32 at 256x256x16, 512x512x16 and on the 2048x2048 Wilson lattice
+    (Ls = 1; one JSON line)."""
     import torch
     import three_part_dwf_study_b200 as T
     from three_part_dwf_study_b200 import _capi as A
     out = {}
-    for lat in ((256, 256, 16), DSLASH_LATTICE):
+    for lat in ((256, 256, 16), DSLASH_LATTICE, WILSON_DSLASH_LATTICE + (1,)):
         Dt, Dx, Dl = lat
-        d = T.DomainWall(Dt, Dx, Dl, M5, MF, BETA)
+        if Dl == 1:
+            d = T.Wilson(Dt, Dx, 0.1, 0.0)
+        else:
+            d = T.DomainWall(Dt, Dx, Dl, M5, MF, BETA)
         d.set_gauge(np.random.default_rng(3).uniform(-np.pi, np.pi, 2 * Dt * Dx))
         st = torch.cuda.ExternalStream(d.stream_ptr())
         for prec, dt, w in ((64, torch.float64, 8), (32, torch.float32, 4)):
             a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
             b = torch.empty_like(a)
-            for v, chunk, name in ((0, 0, "site"), (1, 0, "column"), (2, 0, "site_shuffle"),
-                                   (3, 0, "t_sweep_auto"), (3, 8, "t_sweep_8"),
-                                   (3, 16, "t_sweep_16"), (3, 32, "t_sweep_32"),
-                                   (3, 64, "t_sweep_64")):
+            kinds = [(0, 0, "site"), (1, 0, "column"), (2, 0, "site_shuffle"),
+                     (3, 0, "t_sweep_auto"), (3, 8, "t_sweep_8"), (3, 16, "t_sweep_16"),
+                     (3, 32, "t_sweep_32"), (3, 64, "t_sweep_64")]
+            if Dl == 1:
+                kinds += [(3, 128, "t_sweep_128"), (3, 256, "t_sweep_256"),
+                          (3, 2048, "t_sweep_2048"), (4, 0, "rows")]
+            for v, chunk, name in kinds:
                 A.check(A.lib().dwf_set_dslash_chunk(d.handle, chunk), d.handle)
                 A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
                 for _ in range(3):
@@ -996,9 +1004,11 @@ def dslash_variants():
                 e1.record(st)
                 e1.synchronize()
                 tsec = e0.elapsed_time(e1) * 1e-3 / 20
-                out[f"{Dt}x{Dx}x{Dl}_fp{prec}_{name}"] = round(dslash_bytes(Dt * Dx, Dl, w) / tsec / 1e9, 1)
+                tag = f"wilson_{Dt}x{Dx}" if Dl == 1 else f"{Dt}x{Dx}x{Dl}"
+                out[f"{tag}_fp{prec}_{name}"] = round(dslash_bytes(Dt * Dx, Dl, w) / tsec / 1e9, 1)
         d.close()
-    print(json.dumps({"dslash_GBs": out, "bytes_rule": "V*(Ls*64+32) FP64, V*(Ls*32+16) FP32"}))
+    print(json.dumps({"dslash_GBs": out, "bytes_rule": "V*(Ls*64+32) FP64, V*(Ls*32+16) FP32; "
+                      "Wilson (Ls = 1) V*96 FP64, V*48 FP32"}))
     return 0
 
 

@@ -143,7 +143,8 @@ int dwf_set_gauge_dev(dwf_ctx* ctx, int nconf, const double* theta_dev);
  * (apply_D / apply_D_dagger / apply_DD_dagger / apply_D_dagger_D,
  *  domain_wall/include/dwf_operator.hpp:15-181). */
 int dwf_apply(dwf_ctx* ctx, int op, int conf, const double* in, double* out, int nrhs);
-/* Device version; precision 64 (complex<double>) or 32 (complex<float>). */
+/* Device version; precision 64 (complex<double>) or 32 (complex<float>).
+ * Both fields must start on a 16-byte boundary (DWF_BAD_ARG otherwise). */
 int dwf_apply_dev(dwf_ctx* ctx, int op, int conf, const void* in_dev, void* out_dev, int nrhs,
                   int precision);
 
@@ -344,7 +345,10 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
  * the x neighbours exchanged by warp shuffles (Nx a multiple of 32; else as
  * 0), 3 = one thread per (s, x) sweeping a chunk of rows in t, the rows
  * streamed through a shared-memory ring by cp.async (Nx a multiple of 32 and
- * Ls <= 16; else as 0), -1 = autotune (default): the first application per
+ * Ls <= 16; else as 0), 4 = Wilson contexts only: one thread per four
+ * consecutive rows of one column, all loads up front into registers (Nx a
+ * multiple of 32 and Nt of 4; else as 0), -1 = autotune (default): the first
+ * application per
  * (precision, batch-size bucket) times the variants with CUDA events and
  * keeps the fastest. dwf_dslash_variant reports the choice in force for a
  * precision and batch size (-1 if not tuned yet). */

@@ -199,7 +199,7 @@ def test_bounded_barrier_times_out_and_context_survives(tdwf):
     assert r.converged and r.info["true_relres"] < 1e-9
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("shape", [(8, 8, 4), (13, 37, 3), (64, 64, 16), (5, 3, 1), (16, 40, 24),
                                    (6, 32, 2), (3, 96, 5), (9, 128, 4), (20, 64, 1)])
 def test_dslash_variants_match_oracle(tdwf, variant, shape):
@@ -207,7 +207,8 @@ def test_dslash_variants_match_oracle(tdwf, variant, shape):
     sweeping the fifth dimension; one thread per 5-D site with warp-shuffled x
     neighbours, which takes Nx % 32 == 0 and otherwise runs as the first; one
     thread per (s, x) sweeping a chunk of rows in t, which takes Nx % 32 == 0
-    and Ls <= 16 and otherwise runs as the first) in FP64 and FP32, ragged
+    and Ls <= 16 and otherwise runs as the first; the Wilson-only row kernel,
+    which runs as the first on domain wall) in FP64 and FP32, ragged
     tile edges, row/warp boundaries, several x tiles per block (9x128x4,
     20x64x1) and ragged t chunks included."""
     torch = pytest.importorskip("torch")
@@ -254,12 +255,16 @@ def test_dslash_sweep_chunks(tdwf, chunk, shape):
     assert A.lib().dwf_set_dslash_chunk(d.handle, -1) != 0
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
-@pytest.mark.parametrize("shape", [(16, 256), (7, 96), (12, 64)])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("shape", [(16, 256), (7, 96), (12, 64), (4, 32), (8, 32), (36, 160)])
 def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
     """The Wilson operator (no fifth dimension, antiperiodic in both
-    directions) through every Dslash kernel; 16x256 puts eight 32-x tiles in
-    one block of the t-sweeping kernel."""
+    directions) through every Dslash kernel in FP64 and FP32; 16x256 puts
+    eight 32-x tiles in one block of the t-sweeping kernel; for the row kernel
+    (4 rows per thread, Nt % 4 == 0, else run as the site kernel) 4x32 is one
+    warp whose halo rows and edge lanes both wrap, 7x96 the fallback, and
+    36x160 leaves part of the last block without rows."""
+    torch = pytest.importorskip("torch")
     from three_part_dwf_study_b200 import _capi as A
     Nt, Nx = shape
     rng = np.random.default_rng(Nt + Nx)
@@ -271,9 +276,14 @@ def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
     for op, name in OPS:
         ref = np.concatenate([o.apply(op, th, psi[:o.ntot]), o.apply(op, th, psi[o.ntot:])])
         assert rel(w.apply(op, th, psi), ref) < 1e-13, name
+        x32 = torch.from_numpy(psi.astype(np.complex64)).cuda()
+        y32 = torch.empty_like(x32)
+        w.apply_dev(op, x32, y32)
+        assert rel(y32.cpu().numpy(), ref) < 2e-6, name
+    assert A.lib().dwf_dslash_variant(w.handle, 32, 2) == variant
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_dslash_unaligned_fields(tdwf, variant):
     """FP64 fields that start 16 bytes past a 32-byte boundary (a view one
     complex number into a buffer) take the kernels' 16-byte access path; the
@@ -302,3 +312,21 @@ def test_dslash_unaligned_fields(tdwf, variant):
         ya = torch.empty_like(xa)
         d.apply_dev(op, xa, ya)
         assert rel(ya.cpu().numpy(), ref) < 1e-13, name
+
+
+def test_apply_rejects_fields_off_16_byte_boundary(tdwf):
+    """FP32 fields one complex number into a buffer (8 bytes past a 16-byte
+    boundary) are refused with an error, not read by 16-byte accesses."""
+    torch = pytest.importorskip("torch")
+    from three_part_dwf_study_b200 import _capi as A
+    w = tdwf.Wilson(8, 32, 0.1, 0.0)
+    w.set_gauge(random_theta(np.random.default_rng(3), 8, 32))
+    n = 8 * 32 * 2
+    buf = torch.zeros(n + 1, dtype=torch.complex64, device="cuda")
+    ok = torch.zeros(n, dtype=torch.complex64, device="cuda")
+    assert buf[1:].data_ptr() % 16 == 8
+    with pytest.raises(A.DwfError):
+        w.apply_dev(0, buf[1:], ok)
+    with pytest.raises(A.DwfError):
+        w.apply_dev(0, ok, buf[1:])
+    w.apply_dev(0, buf[:n], ok)

@@ -1,6 +1,7 @@
 // C ABI: contexts, gauge upload, operator application and the batched solver.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -135,6 +136,10 @@ namespace {
 // One application of D (dag = false) or D^dag with the chosen kernel variant.
 // The t-sweeping kernel needs whole 32-lane rows and a block of all Ls slices.
 bool sweep_ok(const Lat& L) { return L.Nx % 32 == 0 && 32 * L.Ls <= 512; }
+bool wilson_rows_ok(const Lat& L)
+{
+    return L.Ls == 1 && !L.fifth && L.Nx % 32 == 0 && L.Nt % kWilsonRows == 0;
+}
 
 struct SweepShape
 {
@@ -204,6 +209,16 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
         }
         kern<<<grid, block, smem, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0, sh.tc);
     }
+    else if (variant == 4 && wilson_rows_ok(c->L))
+    {
+        constexpr int by = 8;
+        const dim3 grid(c->L.Nx / 32, (c->L.Nt / kWilsonRows + by - 1) / by, nrhs);
+        const dim3 block(32, by);
+        if (dag)
+            wilson_rows_kernel<true, R, kWilsonRows><<<grid, block, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        else
+            wilson_rows_kernel<false, R, kWilsonRows><<<grid, block, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+    }
     else if (variant == 1)
     {
         const dim3 grid((c->L.Nx + 31) / 32, (c->L.Nt + 7) / 8, nrhs);
@@ -238,7 +253,8 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
 // context stream) for this precision and batch-size bucket, keep the fastest:
 // 0 one thread per 5-D site, 1 one thread per 4-D column, 2 one thread per 5-D
 // site with warp-shuffled x neighbours (Nx a multiple of 32), 3 one thread per
-// (s, x) sweeping a chunk of rows in t (Nx a multiple of 32, Ls <= 16).
+// (s, x) sweeping a chunk of rows in t (Nx a multiple of 32, Ls <= 16), 4 (Wilson
+// only) one thread per kWilsonRows rows of one column from registers.
 template <typename R>
 int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<R>* in,
                  cplx<R>* out, const cplx<R>* U)
@@ -254,9 +270,10 @@ int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<
         return it->second;
     float best = 1e30f;
     int choice = 0;
-    for (int v = 0; v < 4; ++v)
+    for (int v = 0; v < 5; ++v)
     {
-        if ((v == 2 && c->L.Nx % 32 != 0) || (v == 3 && !sweep_ok(c->L)))
+        if ((v == 2 && c->L.Nx % 32 != 0) || (v == 3 && !sweep_ok(c->L)) ||
+            (v == 4 && !wilson_rows_ok(c->L)))
             continue;
         launch_dirac<R>(c, v, false, nrhs, conf_d, conf0, in, out, U);  // warm-up
         cudaEventRecord(c->ev0, c->stream);
@@ -285,6 +302,9 @@ int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const 
         return ctx_fail(c, DWF_BAD_ARG, "apply: bad op, nrhs or precision");
     if (conf0 < 0 || conf0 >= c->nconf)
         return ctx_fail(c, DWF_BAD_ARG, "apply: configuration index out of range (set_gauge first)");
+    // the kernels move a spin pair (FP32) or a complex number (FP64) per 16-byte access
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15)
+        return ctx_fail(c, DWF_BAD_ARG, "apply: fields must start on a 16-byte boundary");
     const bool two = (op == DWF_OP_DDDAG || op == DWF_OP_DDAGD);
     if (two)
     {
@@ -919,7 +939,7 @@ uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
 
 int dwf_set_dslash_variant(dwf_ctx* c, int variant)
 {
-    if (!c || variant < -1 || variant > 3)
+    if (!c || variant < -1 || variant > 4)
         return DWF_BAD_ARG;
     c->dslash_variant = variant;
     if (variant == -1)

@@ -57,6 +57,32 @@ struct SumLd
     }
 };
 
+// The 4-D hopping sum of one site from its four neighbours' spinors, the
+// links and the boundary signs: D psi = diag psi - (up, lo) / 2 (plus the
+// fifth-dimension hop for domain wall). Forward hops use (1 + kf gamma),
+// backward hops (1 + kb gamma).
+template <bool DAG, typename R>
+__device__ __forceinline__ void hop4(const Spinor<R>& vtp, const Spinor<R>& vtm,
+                                     const Spinor<R>& vxp, const Spinor<R>& vxm, cplx<R> Ut,
+                                     cplx<R> Utm, cplx<R> Ux, cplx<R> Uxm, R stp, R stm, R sxp,
+                                     R sxm, cplx<R>& up, cplx<R>& lo)
+{
+    constexpr R kf = DAG ? R(1) : R(-1);
+    constexpr R kb = -kf;
+    cplx<R> w = cmul(Ut, stp * (vtp.s0 + kf * vtp.s1));
+    up = w;
+    lo = kf * w;
+    w = cmulc(Utm, stm * (vtm.s0 + kb * vtm.s1));
+    up += w;
+    lo += kb * w;
+    w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
+    up += w;
+    lo += kf * itimes(w);
+    w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
+    up += w;
+    lo += kb * itimes(w);
+}
+
 // Link phases are stored per configuration as U[mu][t][x] = (cos, sin).
 template <bool DAG, typename R, typename Ld>
 __device__ __forceinline__ Spinor<R> dirac_site_ld(const Ld& in, const cplx<R>* __restrict__ U,
@@ -85,22 +111,8 @@ __device__ __forceinline__ Spinor<R> dirac_site_ld(const Ld& in, const cplx<R>* 
     const R stm = (t == 0) ? R(L.bct) : R(1);
     const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
     const R sxm = (x == 0) ? R(L.bcx) : R(1);
-    // forward hops use (1 + kf gamma), backward hops (1 + kb gamma)
-    constexpr R kf = DAG ? R(1) : R(-1);
-    constexpr R kb = -kf;
-
-    T w = cmul(Ut, stp * (vtp.s0 + kf * vtp.s1));
-    T up = w;
-    T lo = kf * w;
-    w = cmulc(Utm, stm * (vtm.s0 + kb * vtm.s1));
-    up += w;
-    lo += kb * w;
-    w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
-    up += w;
-    lo += kf * itimes(w);
-    w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
-    up += w;
-    lo += kb * itimes(w);
+    T up, lo;
+    hop4<DAG, R>(vtp, vtm, vxp, vxm, Ut, Utm, Ux, Uxm, stp, stm, sxp, sxm, up, lo);
 
     const R dg = R(L.diag);
     Spinor<R> o;
@@ -187,21 +199,8 @@ __device__ __forceinline__ Spinor<R> dirac_site_warp(const cplx<R>* __restrict__
     const R stm = (t == 0) ? R(L.bct) : R(1);
     const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
     const R sxm = (x == 0) ? R(L.bcx) : R(1);
-    constexpr R kf = DAG ? R(1) : R(-1);
-    constexpr R kb = -kf;
-
-    T w = cmul(Ut, stp * (vtp.s0 + kf * vtp.s1));
-    T upv = w;
-    T lo = kf * w;
-    w = cmulc(Utm, stm * (vtm.s0 + kb * vtm.s1));
-    upv += w;
-    lo += kb * w;
-    w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
-    upv += w;
-    lo += kf * itimes(w);
-    w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
-    upv += w;
-    lo += kb * itimes(w);
+    T upv, lo;
+    hop4<DAG, R>(vtp, vtm, vxp, vxm, Ut, Utm, Ux, Uxm, stp, stm, sxp, sxm, upv, lo);
 
     const R dg = R(L.diag);
     Spinor<R> o;
@@ -263,8 +262,6 @@ __device__ __forceinline__ void dirac_column(const cplx<R>* __restrict__ in,
     const R stm = (t == 0) ? R(L.bct) : R(1);
     const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
     const R sxm = (x == 0) ? R(L.bcx) : R(1);
-    constexpr R kf = DAG ? R(1) : R(-1);
-    constexpr R kb = -kf;
     const R dg = R(L.diag), mf = R(L.mf);
     const Spinor<R> first = ld_spinor(in, here);
     Spinor<R> prev = L.fifth ? ld_spinor(in, long(Ls - 1) * V + here) : first;
@@ -277,18 +274,8 @@ __device__ __forceinline__ void dirac_column(const cplx<R>* __restrict__ in,
         const Spinor<R> vtm = ld_spinor(in, sb + itm);
         const Spinor<R> vxp = ld_spinor(in, sb + ixp);
         const Spinor<R> vxm = ld_spinor(in, sb + ixm);
-        T w = cmul(Ut, stp * (vtp.s0 + kf * vtp.s1));
-        T up = w;
-        T lo = kf * w;
-        w = cmulc(Utm, stm * (vtm.s0 + kb * vtm.s1));
-        up += w;
-        lo += kb * w;
-        w = cmul(Ux, sxp * (vxp.s0 - kf * itimes(vxp.s1)));
-        up += w;
-        lo += kf * itimes(w);
-        w = cmulc(Uxm, sxm * (vxm.s0 - kb * itimes(vxm.s1)));
-        up += w;
-        lo += kb * itimes(w);
+        T up, lo;
+        hop4<DAG, R>(vtp, vtm, vxp, vxm, Ut, Utm, Ux, Uxm, stp, stm, sxp, sxm, up, lo);
         Spinor<R> o{dg * cur.s0 - R(0.5) * up, dg * cur.s1 - R(0.5) * lo};
         if (L.fifth)
         {

@@ -70,6 +70,93 @@ template __global__ void dirac_warp_kernel<false, float>(Lat, const float2*, flo
 template __global__ void dirac_warp_kernel<true, float>(Lat, const float2*, float2*, long,
                                                         const float2*, long, const int*, int);
 
+template <bool DAG, typename R, int RT>
+__global__ void __launch_bounds__(256)
+    wilson_rows_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out, long fsz,
+                       const cplx<R>* __restrict__ U, long usz, const int* __restrict__ conf,
+                       int conf0)
+{
+    using T = cplx<R>;
+    const int j = blockIdx.z;
+    const int c = conf ? conf[j] : conf0;
+    const T* __restrict__ Uj = U + long(c) * usz;
+    const T* __restrict__ inj = in + j * fsz;
+    T* __restrict__ outj = out + j * fsz;
+    const int Nt = L.Nt, Nx = L.Nx, V = L.V;
+    const int lane = threadIdx.x;
+    const int t0 = (blockIdx.y * blockDim.y + threadIdx.y) * RT;
+    if (t0 >= Nt)
+        return;  // the whole warp: t0 is the same for its 32 lanes
+    const int x = blockIdx.x * 32 + lane;
+    const int xp = (x + 1 == Nx) ? 0 : x + 1;
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+
+    // every load up front: rows t0-1 .. t0+RT of this column (t links of
+    // rows t0-1 .. t0+RT-1), the x links of the RT rows, and the neighbour
+    // outside the warp for the edge lanes (x+1 for lane 31, x-1 and its link
+    // for lane 0)
+    Spinor<R> v[RT + 2], h[RT] = {};
+    T ut[RT + 1], ux[RT], uh[RT] = {};
+#pragma unroll
+    for (int k = 0; k < RT + 2; ++k)
+    {
+        int t = t0 - 1 + k;  // in [-1, Nt] since Nt % RT == 0
+        t = (t < 0) ? t + Nt : (t >= Nt ? t - Nt : t);
+        v[k] = ld_spinor(inj, long(t) * Nx + x);
+        if (k <= RT)
+            ut[k] = Uj[t * Nx + x];
+    }
+#pragma unroll
+    for (int k = 0; k < RT; ++k)
+    {
+        const int row = (t0 + k) * Nx;
+        ux[k] = Uj[V + row + x];
+        if (lane == 31)
+            h[k] = ld_spinor(inj, long(row) + xp);
+        if (lane == 0)
+        {
+            h[k] = ld_spinor(inj, long(row) + xm);
+            uh[k] = Uj[V + row + xm];
+        }
+    }
+
+    const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
+    const R sxm = (x == 0) ? R(L.bcx) : R(1);
+    const R dg = R(L.diag);
+    const int lp = (lane + 1) & 31, lm = (lane + 31) & 31;
+#pragma unroll
+    for (int k = 0; k < RT; ++k)
+    {
+        const int t = t0 + k;
+        const Spinor<R>& cc = v[k + 1];
+        Spinor<R> vxp{shfl_c(cc.s0, lp), shfl_c(cc.s1, lp)};
+        Spinor<R> vxm{shfl_c(cc.s0, lm), shfl_c(cc.s1, lm)};
+        T Uxm = shfl_c(ux[k], lm);
+        if (lane == 31)
+            vxp = h[k];
+        if (lane == 0)
+        {
+            vxm = h[k];
+            Uxm = uh[k];
+        }
+        const R stp = (t == Nt - 1) ? R(L.bct) : R(1);
+        const R stm = (t == 0) ? R(L.bct) : R(1);
+        T up, lo;
+        hop4<DAG, R>(v[k + 2], v[k], vxp, vxm, ut[k + 1], ut[k], ux[k], Uxm, stp, stm, sxp, sxm,
+                     up, lo);
+        st_spinor(outj, long(t) * Nx + x, Spinor<R>{dg * cc.s0 - R(0.5) * up, dg * cc.s1 - R(0.5) * lo});
+    }
+}
+
+#define DWFB_WILSON_ROWS(DAG, R)                                                                  \
+    template __global__ void wilson_rows_kernel<DAG, R, kWilsonRows>(                             \
+        Lat, const cplx<R>*, cplx<R>*, long, const cplx<R>*, long, const int*, int);
+DWFB_WILSON_ROWS(false, double)
+DWFB_WILSON_ROWS(true, double)
+DWFB_WILSON_ROWS(false, float)
+DWFB_WILSON_ROWS(true, float)
+#undef DWFB_WILSON_ROWS
+
 // One thread per 4-D site, all Ls slices (links and the fifth-dimension
 // neighbours reused from registers); blocks are 32 x 8 tiles of (x, t) so the
 // t +- 1 neighbours of a warp are mostly loaded by the block's other warps.

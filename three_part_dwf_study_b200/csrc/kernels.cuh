@@ -22,6 +22,18 @@ __global__ void dirac_warp_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>
                                   long fsz, const cplx<R>* __restrict__ U, long usz,
                                   const int* __restrict__ conf, int conf0);
 
+// Wilson only (Ls = 1, no fifth dimension; Nx % 32 == 0, Nt % RT == 0): a
+// warp covers 32 consecutive x of RT consecutive rows, each thread loading
+// its column's rows t0-1 .. t0+RT into registers up front (RT + 2 spinor loads
+// for RT sites), the x neighbours and backward x link by shuffle, the two
+// edge lanes loading theirs (grid: Nx/32 x ceil(Nt/(RT by)) x nrhs, block
+// (32, by)).
+constexpr int kWilsonRows = 4;
+template <bool DAG, typename R, int RT>
+__global__ void wilson_rows_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                                   long fsz, const cplx<R>* __restrict__ U, long usz,
+                                   const int* __restrict__ conf, int conf0);
+
 // Same operator, one thread per 4-D site sweeping the fifth dimension
 // (grid: ceil(Nx/32) x ceil(Nt/8) x nrhs, 256 threads).
 template <bool DAG, typename R>

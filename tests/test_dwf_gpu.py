@@ -283,6 +283,32 @@ def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
     assert A.lib().dwf_dslash_variant(w.handle, 32, 2) == variant
 
 
+def test_wilson_dslash_autotuned_matches_oracle(tdwf):
+    """The autotuner's pick on a 64x512 Wilson lattice (candidates include the
+    t sweep at 16-, 32- and 64-row chunks with 16 and 4 x tiles per block)
+    agrees with the oracle in FP64 and FP32, one and three fields."""
+    torch = pytest.importorskip("torch")
+    from three_part_dwf_study_b200 import _capi as A
+    Nt, Nx = 64, 512
+    rng = np.random.default_rng(64512)
+    w = tdwf.Wilson(Nt, Nx, 0.05, 0.0)
+    o = O.Wilson(Nt, Nx, 0.05, -1.0, 1.0)
+    assert A.lib().dwf_set_dslash_variant(w.handle, -1) == 0
+    th = random_theta(rng, Nt, Nx)
+    for nf in (1, 3):
+        psi = random_field(rng, nf * o.ntot)
+        for op, name in OPS:
+            ref = np.concatenate([o.apply(op, th, psi[k * o.ntot:(k + 1) * o.ntot])
+                                  for k in range(nf)])
+            assert rel(w.apply(op, th, psi), ref) < 1e-13, name
+            x32 = torch.from_numpy(psi.astype(np.complex64)).cuda()
+            y32 = torch.empty_like(x32)
+            w.apply_dev(op, x32, y32)
+            assert rel(y32.cpu().numpy(), ref) < 2e-6, name
+        for prec in (64, 32):
+            assert A.lib().dwf_dslash_variant(w.handle, prec, nf) in (0, 1, 2, 3, 4)
+
+
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_dslash_unaligned_fields(tdwf, variant):
     """FP64 fields that start 16 bytes past a 32-byte boundary (a view one

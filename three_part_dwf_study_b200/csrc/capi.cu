@@ -173,19 +173,35 @@ SweepShape sweep_shape(const dwf_ctx* c, int nrhs, int resident_threads, int rin
     return {g, tc};
 }
 
+using DslashChoice = dwf_ctx::DslashChoice;
+
+// The t-sweeping kernel's compile-time shape per precision.
 template <typename R>
-void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d, int conf0,
+struct SweepCfg
+{
+    static constexpr int NPG = sizeof(R) == 8 ? kSweepGroups64 : kSweepGroups32;
+    static constexpr int RPS = sizeof(R) == 8 ? kSweepRows64 : kSweepRows32;
+    static constexpr int S = sweep_ring_rows(NPG, RPS);
+    // resident threads per SM as the kernel's launch bounds allow
+    static constexpr int resident = (sizeof(R) == 8 && RPS == 2) ? 512 : 1024;
+};
+
+template <typename R>
+SweepShape auto_sweep_shape(const dwf_ctx* c, int nrhs)
+{
+    return sweep_shape(c, nrhs, SweepCfg<R>::resident, SweepCfg<R>::S, sizeof(cplx<R>));
+}
+
+template <typename R>
+void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* conf_d, int conf0,
                   const cplx<R>* in, cplx<R>* out, const cplx<R>* U)
 {
     const long fs = c->fsz();
+    const int variant = ch.variant;
     if (variant == 3 && sweep_ok(c->L))
     {
-        constexpr int NPG = sizeof(R) == 8 ? kSweepGroups64 : kSweepGroups32;
-        constexpr int RPS = sizeof(R) == 8 ? kSweepRows64 : kSweepRows32;
-        constexpr int S = sweep_ring_rows(NPG, RPS);
-        // resident threads per SM as the kernel's launch bounds allow
-        const SweepShape sh = sweep_shape(c, nrhs, (sizeof(R) == 8 && RPS == 2) ? 512 : 1024, S,
-                                          sizeof(cplx<R>));
+        constexpr int NPG = SweepCfg<R>::NPG, RPS = SweepCfg<R>::RPS, S = SweepCfg<R>::S;
+        const SweepShape sh = ch.tc > 0 ? SweepShape{ch.g, ch.tc} : auto_sweep_shape<R>(c, nrhs);
         const dim3 grid(c->L.Nx / (32 * sh.g), (c->L.Nt + sh.tc - 1) / sh.tc, nrhs);
         const dim3 block(32, c->L.Ls, sh.g);
         const size_t smem = S * sweep_slot_bytes(c->L.Ls, sh.g, sizeof(cplx<R>));
@@ -254,13 +270,17 @@ void launch_dirac(dwf_ctx* c, int variant, bool dag, int nrhs, const int* conf_d
 // 0 one thread per 5-D site, 1 one thread per 4-D column, 2 one thread per 5-D
 // site with warp-shuffled x neighbours (Nx a multiple of 32), 3 one thread per
 // (s, x) sweeping a chunk of rows in t (Nx a multiple of 32, Ls <= 16), 4 (Wilson
-// only) one thread per kWilsonRows rows of one column from registers.
+// only) one thread per kWilsonRows rows of one column from registers. Unless
+// the context fixes the chunk length, the t sweep is timed at its automatic
+// shape and at chunks of 16, 32 and 64 rows with the widest block and with a
+// quarter of its 32-x tiles: long chunks amortise the ring's start-up, narrower
+// blocks keep enough of them to fill the SMs.
 template <typename R>
-int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<R>* in,
-                 cplx<R>* out, const cplx<R>* U)
+DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<R>* in,
+                          cplx<R>* out, const cplx<R>* U)
 {
     if (c->dslash_variant >= 0)
-        return c->dslash_variant;
+        return {c->dslash_variant, 0, 0};
     int bucket = 0;
     while ((1 << bucket) < nrhs && bucket < 20)
         ++bucket;
@@ -268,17 +288,34 @@ int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<
     auto it = c->dslash_tuned.find(key);
     if (it != c->dslash_tuned.end())
         return it->second;
-    float best = 1e30f;
-    int choice = 0;
+    std::vector<DslashChoice> cand;
     for (int v = 0; v < 5; ++v)
     {
         if ((v == 2 && c->L.Nx % 32 != 0) || (v == 3 && !sweep_ok(c->L)) ||
             (v == 4 && !wilson_rows_ok(c->L)))
             continue;
-        launch_dirac<R>(c, v, false, nrhs, conf_d, conf0, in, out, U);  // warm-up
+        cand.push_back({v, 0, 0});
+        if (v == 3 && c->dslash_chunk <= 0)
+        {
+            const SweepShape a = auto_sweep_shape<R>(c, nrhs);
+            for (int g : {a.g, std::max(1, a.g / 4)})
+            {
+                for (int tc : {16, 32, 64})
+                    if (tc <= c->L.Nt && !(g == a.g && tc == a.tc))
+                        cand.push_back({3, tc, g});
+                if (a.g < 4)
+                    break;
+            }
+        }
+    }
+    float best = 1e30f;
+    DslashChoice choice = cand.front();
+    for (const DslashChoice& ch : cand)
+    {
+        launch_dirac<R>(c, ch, false, nrhs, conf_d, conf0, in, out, U);  // warm-up
         cudaEventRecord(c->ev0, c->stream);
         for (int k = 0; k < 2; ++k)
-            launch_dirac<R>(c, v, false, nrhs, conf_d, conf0, in, out, U);
+            launch_dirac<R>(c, ch, false, nrhs, conf_d, conf0, in, out, U);
         cudaEventRecord(c->ev1, c->stream);
         cudaEventSynchronize(c->ev1);
         float ms = 0.f;
@@ -286,7 +323,7 @@ int pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<
         if (ms < best)
         {
             best = ms;
-            choice = v;
+            choice = ch;
         }
     }
     c->dslash_tuned[key] = choice;
@@ -318,7 +355,7 @@ int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const 
     {
         const double2* src = static_cast<const double2*>(in);
         double2* mid = two ? c->w_t : static_cast<double2*>(out);
-        const int v = pick_variant<double>(c, nrhs, conf_d, conf0, src, mid, c->U64);
+        const DslashChoice v = pick_variant<double>(c, nrhs, conf_d, conf0, src, mid, c->U64);
         launch_dirac<double>(c, v, dag1, nrhs, conf_d, conf0, src, mid, c->U64);
         if (two)
             launch_dirac<double>(c, v, !dag1, nrhs, conf_d, conf0, mid, static_cast<double2*>(out), c->U64);
@@ -327,7 +364,7 @@ int apply_dev(dwf_ctx* c, int op, int nrhs, const int* conf_d, int conf0, const 
     {
         const float2* src = static_cast<const float2*>(in);
         float2* mid = two ? c->w_t32 : static_cast<float2*>(out);
-        const int v = pick_variant<float>(c, nrhs, conf_d, conf0, src, mid, c->U32);
+        const DslashChoice v = pick_variant<float>(c, nrhs, conf_d, conf0, src, mid, c->U32);
         launch_dirac<float>(c, v, dag1, nrhs, conf_d, conf0, src, mid, c->U32);
         if (two)
             launch_dirac<float>(c, v, !dag1, nrhs, conf_d, conf0, mid, static_cast<float2*>(out), c->U32);
@@ -966,7 +1003,7 @@ int dwf_dslash_variant(const dwf_ctx* c, int precision, int nrhs)
     while ((1 << bucket) < nrhs && bucket < 20)
         ++bucket;
     const auto it = c->dslash_tuned.find((precision == 64 ? 100 : 0) + bucket);
-    return it == c->dslash_tuned.end() ? -1 : it->second;
+    return it == c->dslash_tuned.end() ? -1 : it->second.variant;
 }
 
 int dwf_barrier_selftest(dwf_ctx* c, int missing_blocks, uint64_t limit_ns)

@@ -22,13 +22,20 @@ struct dwf_ctx
     uint64_t gauge_version = 0;  // bumped whenever the links change
     struct LpNet* lp = nullptr;  // learned preconditioner (dwf_lp_init)
     uint64_t launches = 0;  // kernels launched by this context
-    // Dslash kernel variant: -1 autotune, 0 one thread per 5-D site, 1 one
-    // thread per 4-D site sweeping the fifth dimension; tuned choices cached
-    // per (precision, batch-size bucket).
+    // Dslash kernel variant (-1 autotune, 0-4 as dwf_set_dslash_variant
+    // lists them); tuned choices cached per (precision, batch-size bucket),
+    // for the t-sweeping kernel with its chunk length and 32-x tiles per block
+    // (0: the automatic shape).
+    struct DslashChoice
+    {
+        int variant = 0;
+        int tc = 0;
+        int g = 0;
+    };
     int dslash_variant = -1;
     int dslash_chunk = 0;    // rows per chunk of the t-sweeping Dslash (0 = automatic)
     int sweep_smem_set = 0;  // t-sweeping kernels whose shared-memory limit is raised (bits)
-    std::map<int, int> dslash_tuned;
+    std::map<int, DslashChoice> dslash_tuned;
     // CUDA events bracketing each persistent solver launch on `stream`
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double solver_ms[2] = {0.0, 0.0};  // device time of solver launches: full lattice, even-odd

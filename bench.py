@@ -921,6 +921,29 @@ def profile_dslash():
     return 0
 
 
+def profile_wilson_dslash():
+    """The Wilson operator alone at 2048x2048 (for ncu), one application per
+    precision with the kernels the CUDA-event timing favours: FP64 the site
+    kernel (variant 0), FP32 the t sweep at 64-row chunks (variant 3). The
+    kernels are fixed rather than tuned because ncu's serialised launches
+    would change the autotuner's timing."""
+    import torch
+    import three_part_dwf_study_b200 as T
+    from three_part_dwf_study_b200 import _capi as A
+    Nt, Nx = WILSON_DSLASH_LATTICE
+    w = T.Wilson(Nt, Nx, 0.1, 0.0)
+    w.set_gauge(np.random.default_rng(4).uniform(-np.pi, np.pi, 2 * Nt * Nx))
+    for dt, v, chunk in ((torch.float64, 0, 0), (torch.float32, 3, 64)):
+        A.check(A.lib().dwf_set_dslash_variant(w.handle, v), w.handle)
+        A.check(A.lib().dwf_set_dslash_chunk(w.handle, chunk), w.handle)
+        a = torch.randn(w.Ndof * 2, dtype=dt, device="cuda")
+        b = torch.empty_like(a)
+        w.apply_dev(0, a, b)
+    w.sync()
+    w.close()
+    return 0
+
+
 def profile_network():
     """Network applications only (for ncu captures of the layer kernel): the
     bench's 32-channel network with its initial weights on the workload
@@ -1032,6 +1055,7 @@ def main():
     ap.add_argument("--profile-dslash", action="store_true")
     ap.add_argument("--profile-learned", action="store_true")
     ap.add_argument("--profile-network", action="store_true")
+    ap.add_argument("--profile-wilson-dslash", action="store_true")
     ap.add_argument("--dslash-variants", action="store_true")
     ap.add_argument("--eo-phases", action="store_true")
     args = ap.parse_args()
@@ -1043,6 +1067,8 @@ def main():
         return profile_learned()
     if args.profile_network:
         return profile_network()
+    if args.profile_wilson_dslash:
+        return profile_wilson_dslash()
     if args.dslash_variants:
         return dslash_variants()
     if args.eo_phases:

@@ -350,8 +350,8 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
  * multiple of 32 and Nt of 4; else as 0), -1 = autotune (default): the first
  * application per (precision, batch-size bucket) times the variants with
  * CUDA events and keeps the fastest, variant 3 at its automatic shape and at
- * chunks of 16, 32 and 64 rows with the widest and a quarter-width block
- * (unless dwf_set_dslash_chunk fixes the chunk). dwf_dslash_variant reports the choice in force for a
+ * chunks of 16, 32, 64 and 128 rows with the widest, a half- and a
+ * quarter-width block (unless dwf_set_dslash_chunk fixes the chunk). dwf_dslash_variant reports the choice in force for a
  * precision and batch size (-1 if not tuned yet). */
 int dwf_set_dslash_variant(dwf_ctx* ctx, int variant);
 int dwf_dslash_variant(const dwf_ctx* ctx, int precision, int nrhs);

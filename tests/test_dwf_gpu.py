@@ -285,7 +285,7 @@ def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
 
 def test_wilson_dslash_autotuned_matches_oracle(tdwf):
     """The autotuner's pick on a 64x512 Wilson lattice (candidates include the
-    t sweep at 16-, 32- and 64-row chunks with 16 and 4 x tiles per block)
+    t sweep at 16-, 32- and 64-row chunks with 16, 8 and 4 x tiles per block)
     agrees with the oracle in FP64 and FP32, one and three fields."""
     torch = pytest.importorskip("torch")
     from three_part_dwf_study_b200 import _capi as A

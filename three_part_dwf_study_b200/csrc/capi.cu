@@ -272,9 +272,9 @@ void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* co
 // (s, x) sweeping a chunk of rows in t (Nx a multiple of 32, Ls <= 16), 4 (Wilson
 // only) one thread per kWilsonRows rows of one column from registers. Unless
 // the context fixes the chunk length, the t sweep is timed at its automatic
-// shape and at chunks of 16, 32 and 64 rows with the widest block and with a
-// quarter of its 32-x tiles: long chunks amortise the ring's start-up, narrower
-// blocks keep enough of them to fill the SMs.
+// shape and at chunks of 16, 32, 64 and 128 rows with the widest block and
+// with a half and a quarter of its 32-x tiles: long chunks amortise the ring's
+// start-up, narrower blocks keep enough of them to fill the SMs.
 template <typename R>
 DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, const cplx<R>* in,
                           cplx<R>* out, const cplx<R>* U)
@@ -298,14 +298,10 @@ DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, co
         if (v == 3 && c->dslash_chunk <= 0)
         {
             const SweepShape a = auto_sweep_shape<R>(c, nrhs);
-            for (int g : {a.g, std::max(1, a.g / 4)})
-            {
-                for (int tc : {16, 32, 64})
+            for (int g = a.g; g >= 1 && g * 4 >= a.g; g /= 2)
+                for (int tc : {16, 32, 64, 128})
                     if (tc <= c->L.Nt && !(g == a.g && tc == a.tc))
                         cand.push_back({3, tc, g});
-                if (a.g < 4)
-                    break;
-            }
         }
     }
     float best = 1e30f;

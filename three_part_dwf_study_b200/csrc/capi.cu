@@ -773,7 +773,7 @@ int dwf_ctx_destroy(dwf_ctx* c)
                     c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar,
                     c->eo_se, c->eo_so, c->eo_bh, c->eo_rhs_o, c->eo_x, c->eo_r, c->eo_t, c->eo_y,
                     c->eo_xn, c->eo_r32, c->eo_p32, c->eo_t32, c->eo_y32, c->eo_e32,
-                    c->eo_phase};
+                    c->eo_phase, c->m_red, c->m_loop, c->m_z4};
     for (void* b : bufs)
         if (b)
             cudaFree(b);

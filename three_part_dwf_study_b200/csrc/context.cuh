@@ -64,6 +64,14 @@ struct dwf_ctx
     double* w_part = nullptr;
     size_t w_part_cap = 0;
     double2* w_src = nullptr;  // propagator sources (device staging)
+    // dwf_measure's contraction partials, noise-loop sums and Z4 digits
+    // (grow-only, like the solver workspace)
+    double* m_red = nullptr;
+    size_t m_red_cap = 0;
+    double2* m_loop = nullptr;
+    size_t m_loop_cap = 0;
+    signed char* m_z4 = nullptr;
+    size_t m_z4_cap = 0;
     int* w_conf = nullptr;
     int* w_active = nullptr;
     int* w_iters = nullptr;

@@ -181,22 +181,22 @@ __global__ void loop_kernel(Lat L, int R, int first_noise, int n_noise, long nco
 
 namespace {
 
-struct MeasBuffers
+// Grow-only device buffer of the context (freed by dwf_ctx_destroy).
+template <typename T>
+int reserve(dwf_ctx* c, T*& p, size_t& cap, size_t n)
 {
-    double2* src = nullptr;
-    double2* x = nullptr;
-    double* red = nullptr;
-    signed char* z4 = nullptr;
-    double2* loop = nullptr;
-    void release()
-    {
-        cudaFree(src);
-        cudaFree(x);
-        cudaFree(red);
-        cudaFree(z4);
-        cudaFree(loop);
-    }
-};
+    n = std::max<size_t>(n, 1);
+    if (p && n <= cap)
+        return DWF_OK;
+    CK(cudaStreamSynchronize(c->stream));
+    if (p)
+        cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    CK(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)));
+    cap = n;
+    return DWF_OK;
+}
 
 }  // namespace
 
@@ -224,21 +224,25 @@ int dwf_measure(dwf_ctx* c, const dwf_measure_params* mp, int nconf, const doubl
     const long fs = c->fsz();
     const int nmom = mp->n_point_times > 0 ? mp->max_momentum + 1 : 0;
     const int K = 2 + nmom;
-    MeasBuffers B;
-    auto fail = [&](int code) {
-        B.release();
-        return code;
-    };
-    if (cudaMalloc(&B.src, nrhs * fs * sizeof(double2)) != cudaSuccess ||
-        cudaMalloc(&B.x, nrhs * fs * sizeof(double2)) != cudaSuccess ||
-        cudaMalloc(&B.red, nrhs * c->L.Nt * K * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&B.loop, long(nconf) * c->L.V * sizeof(double2)) != cudaSuccess ||
-        cudaMalloc(&B.z4, std::max<long>(1, long(nconf) * mp->n_noise * c->L.V * 2)) != cudaSuccess)
-        return fail(ctx_fail(c, DWF_CUDA_ERROR, "measure: device allocation failed"));
+    // sources and solutions in the solver workspace's staging fields, the rest
+    // in the context's measurement buffers: no allocation once they have grown
+    if ((st = ensure_workspace(c, int(nrhs))) ||
+        (st = reserve(c, c->m_red, c->m_red_cap, size_t(nrhs) * c->L.Nt * K)) ||
+        (st = reserve(c, c->m_loop, c->m_loop_cap, size_t(nconf) * c->L.V)) ||
+        (st = reserve(c, c->m_z4, c->m_z4_cap, size_t(nconf) * mp->n_noise * c->L.V * 2)))
+        return st;
+    struct
+    {
+        double2* src;
+        double2* x;
+        double* red;
+        signed char* z4;
+        double2* loop;
+    } B{c->w_src, c->w_x, c->m_red, c->m_z4, c->m_loop};
     if (mp->n_noise > 0 &&
         cudaMemcpyAsync(B.z4, z4, long(nconf) * mp->n_noise * c->L.V * 2, cudaMemcpyHostToDevice,
                         c->stream) != cudaSuccess)
-        return fail(ctx_fail(c, DWF_CUDA_ERROR, "measure: z4 upload failed"));
+        return ctx_fail(c, DWF_CUDA_ERROR, "measure: z4 upload failed");
     SrcDesc sd{};
     sd.L = c->L;
     sd.R = R;
@@ -257,7 +261,7 @@ int dwf_measure(dwf_ctx* c, const dwf_measure_params* mp, int nconf, const doubl
     st = propagators(c, int(nrhs), conf.data(), B.src, B.x, mp->rtol, mp->maxiter, mp->solver,
                      inf.data());
     if (st)
-        return fail(st);
+        return st;
     for (long j = 0; j < nrhs; j += 65535)
     {
         const int n = int(std::min<long>(65535, nrhs - j));
@@ -273,15 +277,14 @@ int dwf_measure(dwf_ctx* c, const dwf_measure_params* mp, int nconf, const doubl
         c->launches += 1;
     }
     if (cudaGetLastError() != cudaSuccess)
-        return fail(ctx_fail(c, DWF_CUDA_ERROR, "measure: kernel launch failed"));
+        return ctx_fail(c, DWF_CUDA_ERROR, "measure: kernel launch failed");
     std::vector<double> red(nrhs * c->L.Nt * K);
     std::vector<double> lp(mp->n_noise > 0 ? 2L * nconf * c->L.V : 0);
     cudaMemcpyAsync(red.data(), B.red, red.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (!lp.empty())
         cudaMemcpyAsync(lp.data(), B.loop, lp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess)
-        return fail(ctx_fail(c, DWF_CUDA_ERROR, "measure: copy-back failed"));
-    B.release();
+        return ctx_fail(c, DWF_CUDA_ERROR, "measure: copy-back failed");
 
     const int Nt = c->L.Nt;
     auto R_at = [&](long j, int t, int k) { return red[(j * Nt + t) * K + k]; };
@@ -365,30 +368,26 @@ int wil_pseudoscalar_correlator(dwf_ctx* c, int nconf, const double* thetas, int
         return st;
     const long nrhs = 2L * nconf;
     const long fs = c->fsz();
-    MeasBuffers B;
-    auto fail = [&](int code) {
-        B.release();
-        return code;
-    };
-    if (cudaMalloc(&B.src, nrhs * fs * sizeof(double2)) != cudaSuccess ||
-        cudaMalloc(&B.x, nrhs * fs * sizeof(double2)) != cudaSuccess ||
-        cudaMalloc(&B.red, nrhs * c->L.Nt * 2 * sizeof(double)) != cudaSuccess)
-        return fail(ctx_fail(c, DWF_CUDA_ERROR, "correlator: device allocation failed"));
+    if ((st = ensure_workspace(c, int(nrhs))) ||
+        (st = reserve(c, c->m_red, c->m_red_cap, size_t(nrhs) * c->L.Nt * 2)))
+        return st;
+    double2* const src = c->w_src;
+    double2* const x = c->w_x;
     SrcDesc sd{};
     sd.L = c->L;
     sd.R = 2;
     sd.ls_src = 0;
     sd.src_x = src_x;
     sd.wil_t = src_t;
-    sources_kernel<<<std::max(1, 8 * c->nsm), 256, 0, c->stream>>>(sd, nrhs, B.src);
+    sources_kernel<<<std::max(1, 8 * c->nsm), 256, 0, c->stream>>>(sd, nrhs, src);
     c->launches += 1;
     std::vector<int> conf(nrhs);
     for (long j = 0; j < nrhs; ++j)
         conf[j] = int(j / 2);
     std::vector<dwf_solve_info> inf(nrhs);
-    st = propagators(c, int(nrhs), conf.data(), B.src, B.x, tol, maxiter, solver, inf.data());
+    st = propagators(c, int(nrhs), conf.data(), src, x, tol, maxiter, solver, inf.data());
     if (st)
-        return fail(st);
+        return st;
     for (long j = 0; j < nrhs; ++j)
         if (!std::isfinite(inf[j].true_relres) || inf[j].true_relres > 20.0 * tol)
         {
@@ -396,20 +395,19 @@ int wil_pseudoscalar_correlator(dwf_ctx* c, int nconf, const double* thetas, int
             std::snprintf(msg, sizeof msg,
                           "CGNR failed: iterations=%d, normal residual=%e, D residual=%e",
                           inf[j].iterations, inf[j].true_relres, inf[j].dirac_relres);
-            return fail(ctx_fail(c, DWF_NOT_CONVERGED, msg));
+            return ctx_fail(c, DWF_NOT_CONVERGED, msg);
         }
     for (long j = 0; j < nrhs; j += 65535)
     {
         const int n = int(std::min<long>(65535, nrhs - j));
         contract_kernel<<<dim3(c->L.Nt, n), 128, 2 * c->L.Nx * sizeof(double), c->stream>>>(
-            c->L, 0, 0, B.x + j * fs, B.red + j * c->L.Nt * 2);
+            c->L, 0, 0, x + j * fs, c->m_red + j * c->L.Nt * 2);
         c->launches += 1;
     }
     std::vector<double> red(nrhs * c->L.Nt * 2);
-    cudaMemcpyAsync(red.data(), B.red, red.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    cudaMemcpyAsync(red.data(), c->m_red, red.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess)
-        return fail(ctx_fail(c, DWF_CUDA_ERROR, "correlator: copy-back failed"));
-    B.release();
+        return ctx_fail(c, DWF_CUDA_ERROR, "correlator: copy-back failed");
     for (int cf = 0; cf < nconf; ++cf)
         for (int t = 0; t < c->L.Nt; ++t)
             corr[long(cf) * c->L.Nt + t] =

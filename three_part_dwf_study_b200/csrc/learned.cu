@@ -2682,8 +2682,12 @@ int dwf_lp_train(dwf_ctx* c, const dwf_lp_train_params* tp, dwf_lp_train_info* t
     ST(lp_ensure_act(c, B));
     float2* brho = nullptr;
     float2* be = nullptr;
-    CK(cudaMalloc(&brho, size_t(B) * fs * sizeof(float2)));
-    CK(cudaMalloc(&be, size_t(B) * fs * sizeof(float2)));
+    if (cudaMalloc(&brho, size_t(B) * fs * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&be, size_t(B) * fs * sizeof(float2)) != cudaSuccess)
+    {
+        cudaFree(brho);  // cudaFree(nullptr) is a no-op
+        return ctx_fail(c, DWF_CUDA_ERROR, "dwf_lp_train: mini-batch allocation failed");
+    }
     double first = -1.0, last = -1.0;
     int pos = np;
     std::vector<int> bc(B);

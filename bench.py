@@ -902,8 +902,8 @@ def profile_learned():
 
 def profile_dslash():
     """One application of D at the Dslash bench lattice for each kernel
-    variant (site, column, site with shuffled x neighbours, t sweep) in FP64,
-    then in FP32 (for ncu)."""
+    variant (site, column, site with shuffled x neighbours, t sweep, column
+    with shuffled x neighbours) in FP64, then in FP32 (for ncu)."""
     import torch
     import three_part_dwf_study_b200 as T
     from three_part_dwf_study_b200 import _capi as A
@@ -913,7 +913,7 @@ def profile_dslash():
     for dt in (torch.float64, torch.float32):
         a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
         b = torch.empty_like(a)
-        for v in (0, 1, 2, 3):
+        for v in (0, 1, 2, 3, 5):
             A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
             d.apply_dev(0, a, b)
     d.sync()
@@ -1007,7 +1007,7 @@ def dslash_variants():
         for prec, dt, w in ((64, torch.float64, 8), (32, torch.float32, 4)):
             a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
             b = torch.empty_like(a)
-            kinds = [(0, 0, "site"), (1, 0, "column"), (2, 0, "site_shuffle"),
+            kinds = [(0, 0, "site"), (1, 0, "column"), (2, 0, "site_shuffle"), (5, 0, "column_shuffle"),
                      (3, 0, "t_sweep_auto"), (3, 8, "t_sweep_8"), (3, 16, "t_sweep_16"),
                      (3, 32, "t_sweep_32"), (3, 64, "t_sweep_64")]
             if Dl == 1:

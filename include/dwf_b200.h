@@ -347,7 +347,9 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
  * streamed through a shared-memory ring by cp.async (Nx a multiple of 32 and
  * Ls <= 16; else as 0), 4 = Wilson contexts only: one thread per four
  * consecutive rows of one column, all loads up front into registers (Nx a
- * multiple of 32 and Nt of 4; else as 0), -1 = autotune (default): the first
+ * multiple of 32 and Nt of 4; else as 0), 5 = as 1 with the x neighbours
+ * exchanged by warp shuffles and the next slice's loads issued ahead (Nx a
+ * multiple of 32; else as 1), -1 = autotune (default): the first
  * application per (precision, batch-size bucket) times the variants with
  * CUDA events and keeps the fastest, variant 3 at its automatic shape and at
  * chunks of 16, 32, 64 and 128 rows with the widest, a half- and a

@@ -199,7 +199,7 @@ def test_bounded_barrier_times_out_and_context_survives(tdwf):
     assert r.converged and r.info["true_relres"] < 1e-9
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("shape", [(8, 8, 4), (13, 37, 3), (64, 64, 16), (5, 3, 1), (16, 40, 24),
                                    (6, 32, 2), (3, 96, 5), (9, 128, 4), (20, 64, 1)])
 def test_dslash_variants_match_oracle(tdwf, variant, shape):
@@ -208,7 +208,9 @@ def test_dslash_variants_match_oracle(tdwf, variant, shape):
     neighbours, which takes Nx % 32 == 0 and otherwise runs as the first; one
     thread per (s, x) sweeping a chunk of rows in t, which takes Nx % 32 == 0
     and Ls <= 16 and otherwise runs as the first; the Wilson-only row kernel,
-    which runs as the first on domain wall) in FP64 and FP32, ragged
+    which runs as the first on domain wall; the column kernel with shuffled x
+    neighbours, which takes Nx % 32 == 0 and otherwise runs as the second) in
+    FP64 and FP32, ragged
     tile edges, row/warp boundaries, several x tiles per block (9x128x4,
     20x64x1) and ragged t chunks included."""
     torch = pytest.importorskip("torch")
@@ -255,7 +257,7 @@ def test_dslash_sweep_chunks(tdwf, chunk, shape):
     assert A.lib().dwf_set_dslash_chunk(d.handle, -1) != 0
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("shape", [(16, 256), (7, 96), (12, 64), (4, 32), (8, 32), (36, 160)])
 def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
     """The Wilson operator (no fifth dimension, antiperiodic in both
@@ -306,10 +308,10 @@ def test_wilson_dslash_autotuned_matches_oracle(tdwf):
             w.apply_dev(op, x32, y32)
             assert rel(y32.cpu().numpy(), ref) < 2e-6, name
         for prec in (64, 32):
-            assert A.lib().dwf_dslash_variant(w.handle, prec, nf) in (0, 1, 2, 3, 4)
+            assert A.lib().dwf_dslash_variant(w.handle, prec, nf) in (0, 1, 2, 3, 4, 5)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_dslash_unaligned_fields(tdwf, variant):
     """FP64 fields that start 16 bytes past a 32-byte boundary (a view one
     complex number into a buffer) take the kernels' 16-byte access path; the

@@ -235,7 +235,15 @@ void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* co
         else
             wilson_rows_kernel<false, R, kWilsonRows><<<grid, block, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
     }
-    else if (variant == 1)
+    else if (variant == 5 && c->L.Nx % 32 == 0)
+    {
+        const dim3 grid(c->L.Nx / 32, (c->L.Nt + 7) / 8, nrhs);
+        if (dag)
+            dirac_colx_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        else
+            dirac_colx_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+    }
+    else if (variant == 1 || variant == 5)
     {
         const dim3 grid((c->L.Nx + 31) / 32, (c->L.Nt + 7) / 8, nrhs);
         if (dag)
@@ -270,7 +278,8 @@ void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* co
 // 0 one thread per 5-D site, 1 one thread per 4-D column, 2 one thread per 5-D
 // site with warp-shuffled x neighbours (Nx a multiple of 32), 3 one thread per
 // (s, x) sweeping a chunk of rows in t (Nx a multiple of 32, Ls <= 16), 4 (Wilson
-// only) one thread per kWilsonRows rows of one column from registers. Unless
+// only) one thread per kWilsonRows rows of one column from registers, 5 one
+// thread per 4-D column with warp-shuffled x neighbours (Nx a multiple of 32). Unless
 // the context fixes the chunk length, the t sweep is timed at its automatic
 // shape and at chunks of 16, 32, 64 and 128 rows with the widest block and
 // with a half and a quarter of its 32-x tiles: long chunks amortise the ring's
@@ -289,9 +298,9 @@ DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, co
     if (it != c->dslash_tuned.end())
         return it->second;
     std::vector<DslashChoice> cand;
-    for (int v = 0; v < 5; ++v)
+    for (int v = 0; v < 6; ++v)
     {
-        if ((v == 2 && c->L.Nx % 32 != 0) || (v == 3 && !sweep_ok(c->L)) ||
+        if (((v == 2 || v == 5) && c->L.Nx % 32 != 0) || (v == 3 && !sweep_ok(c->L)) ||
             (v == 4 && !wilson_rows_ok(c->L)))
             continue;
         cand.push_back({v, 0, 0});
@@ -972,7 +981,7 @@ uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
 
 int dwf_set_dslash_variant(dwf_ctx* c, int variant)
 {
-    if (!c || variant < -1 || variant > 4)
+    if (!c || variant < -1 || variant > 5)
         return DWF_BAD_ARG;
     c->dslash_variant = variant;
     if (variant == -1)

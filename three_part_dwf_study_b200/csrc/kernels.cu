@@ -178,6 +178,109 @@ __global__ void __launch_bounds__(256)
                          [&](int s, const Spinor<R>& o) { st_spinor(outj, long(s) * L.V + here, o); });
 }
 
+template <bool DAG, typename R>
+__global__ void __launch_bounds__(256)
+    dirac_colx_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out, long fsz,
+                      const cplx<R>* __restrict__ U, long usz, const int* __restrict__ conf,
+                      int conf0)
+{
+    using T = cplx<R>;
+    const int j = blockIdx.z;
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (t >= L.Nt)
+        return;  // the whole warp: t is the same for its 32 lanes
+    const int c = conf ? conf[j] : conf0;
+    const T* __restrict__ Uj = U + long(c) * usz;
+    const T* __restrict__ inj = in + j * fsz;
+    T* __restrict__ outj = out + j * fsz;
+    const int Nt = L.Nt, Nx = L.Nx, V = L.V, Ls = L.Ls;
+    const int x = blockIdx.x * 32 + lane;
+    const int tp = (t + 1 == Nt) ? 0 : t + 1;
+    const int tm = (t == 0) ? Nt - 1 : t - 1;
+    const int xp = (x + 1 == Nx) ? 0 : x + 1;
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+    const int here = t * Nx + x, itp = tp * Nx + x, itm = tm * Nx + x;
+    // the neighbour outside the warp: x+1 for lane 31, x-1 for lane 0
+    const int ie = t * Nx + ((lane == 31) ? xp : xm);
+    const bool edge = (lane == 0) || (lane == 31);
+    const int lp = (lane + 1) & 31, lm = (lane + 31) & 31;
+
+    const T Ut = Uj[here];
+    const T Utm = Uj[itm];
+    const T Ux = Uj[V + here];
+    T Uxm = shfl_c(Ux, lm);
+    if (lane == 0)
+        Uxm = Uj[V + t * Nx + xm];
+    const R stp = (t == Nt - 1) ? R(L.bct) : R(1);
+    const R stm = (t == 0) ? R(L.bct) : R(1);
+    const R sxp = (x == Nx - 1) ? R(L.bcx) : R(1);
+    const R sxm = (x == 0) ? R(L.bcx) : R(1);
+    const R dg = R(L.diag), mf = R(L.mf);
+
+    // slice s's operands are loaded one slice ahead, before slice s - 1 is computed
+    const Spinor<R> first = ld_spinor(inj, here);
+    Spinor<R> prev = L.fifth ? ld_spinor(inj, long(Ls - 1) * V + here) : first;
+    Spinor<R> cur = first;
+    Spinor<R> vtp = ld_spinor(inj, itp), vtm = ld_spinor(inj, itm), h = {};
+    if (edge)
+        h = ld_spinor(inj, ie);
+    for (int s = 0; s < Ls; ++s)
+    {
+        Spinor<R> nxt = first, ntp = {}, ntm = {}, nh = {};
+        if (s + 1 < Ls)
+        {
+            const long sb = long(s + 1) * V;
+            nxt = ld_spinor(inj, sb + here);
+            ntp = ld_spinor(inj, sb + itp);
+            ntm = ld_spinor(inj, sb + itm);
+            if (edge)
+                nh = ld_spinor(inj, sb + ie);
+        }
+        Spinor<R> vxp{shfl_c(cur.s0, lp), shfl_c(cur.s1, lp)};
+        Spinor<R> vxm{shfl_c(cur.s0, lm), shfl_c(cur.s1, lm)};
+        if (lane == 31)
+            vxp = h;
+        if (lane == 0)
+            vxm = h;
+        T up, lo;
+        hop4<DAG, R>(vtp, vtm, vxp, vxm, Ut, Utm, Ux, Uxm, stp, stm, sxp, sxm, up, lo);
+        Spinor<R> o{dg * cur.s0 - R(0.5) * up, dg * cur.s1 - R(0.5) * lo};
+        if (L.fifth)
+        {
+            // D: spin 1 from s+1 (m_f psi(0) at the top), spin 0 from s-1 (m_f psi(Ls-1)
+            // at 0); D^dag: the directions swapped
+            const R cup = (s + 1 == Ls) ? mf : R(-1);
+            const R cdn = (s == 0) ? mf : R(-1);
+            if (!DAG)
+            {
+                o.s1 += cup * nxt.s1;
+                o.s0 += cdn * prev.s0;
+            }
+            else
+            {
+                o.s1 += cdn * prev.s1;
+                o.s0 += cup * nxt.s0;
+            }
+        }
+        st_spinor(outj, long(s) * V + here, o);
+        prev = cur;
+        cur = nxt;
+        vtp = ntp;
+        vtm = ntm;
+        h = nh;
+    }
+}
+
+#define DWFB_COLX(DAG, R)                                                                         \
+    template __global__ void dirac_colx_kernel<DAG, R>(Lat, const cplx<R>*, cplx<R>*, long,       \
+                                                       const cplx<R>*, long, const int*, int);
+DWFB_COLX(false, double)
+DWFB_COLX(true, double)
+DWFB_COLX(false, float)
+DWFB_COLX(true, float)
+#undef DWFB_COLX
+
 template __global__ void dirac_col_kernel<false, double>(Lat, const double2*, double2*, long,
                                                          const double2*, long, const int*, int);
 template __global__ void dirac_col_kernel<true, double>(Lat, const double2*, double2*, long,

@@ -22,6 +22,16 @@ __global__ void dirac_warp_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>
                                   long fsz, const cplx<R>* __restrict__ U, long usz,
                                   const int* __restrict__ conf, int conf0);
 
+// Same operator, one thread per 4-D site sweeping s like dirac_col_kernel,
+// with the x neighbours and the backward x link exchanged by warp shuffles
+// (Nx % 32 == 0; the two edge lanes load theirs) and slice s+1's spinor loads
+// issued before slice s is computed (grid: Nx/32 x ceil(Nt/8) x nrhs, 256
+// threads, one t row per warp).
+template <bool DAG, typename R>
+__global__ void dirac_colx_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                                  long fsz, const cplx<R>* __restrict__ U, long usz,
+                                  const int* __restrict__ conf, int conf0);
+
 // Wilson only (Ls = 1, no fifth dimension; Nx % 32 == 0, Nt % RT == 0): a
 // warp covers 32 consecutive x of RT consecutive rows, each thread loading
 // its column's rows t0-1 .. t0+RT into registers up front (RT + 2 spinor loads

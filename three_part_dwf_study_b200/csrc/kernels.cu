@@ -178,6 +178,16 @@ __global__ void __launch_bounds__(256)
                          [&](int s, const Spinor<R>& o) { st_spinor(outj, long(s) * L.V + here, o); });
 }
 
+// Slices of lookahead that dirac_colx_kernel prefetches into L1 (0: none).
+#ifndef DWFB_COLX_PREFETCH
+#define DWFB_COLX_PREFETCH 2
+#endif
+
+__device__ __forceinline__ void prefetch_l1(const void* p)
+{
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 template <bool DAG, typename R>
 __global__ void __launch_bounds__(256)
     dirac_colx_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out, long fsz,
@@ -227,6 +237,14 @@ __global__ void __launch_bounds__(256)
         h = ld_spinor(inj, ie);
     for (int s = 0; s < Ls; ++s)
     {
+        if (DWFB_COLX_PREFETCH > 0 && s + DWFB_COLX_PREFETCH < Ls)
+        {
+            // pull slice s + DWFB_COLX_PREFETCH into L1 without holding registers for it
+            const T* const pb = inj + 2 * long(s + DWFB_COLX_PREFETCH) * V;
+            prefetch_l1(pb + 2 * here);
+            prefetch_l1(pb + 2 * itp);
+            prefetch_l1(pb + 2 * itm);
+        }
         Spinor<R> nxt = first, ntp = {}, ntm = {}, nh = {};
         if (s + 1 < Ls)
         {

@@ -192,6 +192,26 @@ SweepShape auto_sweep_shape(const dwf_ctx* c, int nrhs)
     return sweep_shape(c, nrhs, SweepCfg<R>::resident, SweepCfg<R>::S, sizeof(cplx<R>));
 }
 
+// The kernels that use no shared memory lean on L1 for their neighbour reuse
+// (and the column kernel for its prefetched slices). Without a preference the
+// driver may keep a small-L1 split chosen for a preceding shared-memory-heavy
+// kernel (the t sweep, the network layers), so ask once per kernel for the
+// largest L1; a refusal only leaves the default split.
+template <typename K>
+void prefer_l1(dwf_ctx* c, int bit, K kern)
+{
+    if (c->l1_pref_set & (1 << bit))
+        return;
+    // a refusal is not an error of the launch that follows: clear it, unless an
+    // earlier error is pending for the caller's check
+    const bool clean = cudaPeekAtLastError() == cudaSuccess;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             int(cudaSharedmemCarveoutMaxL1)) != cudaSuccess &&
+        clean)
+        cudaGetLastError();
+    c->l1_pref_set |= 1 << bit;
+}
+
 template <typename R>
 void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* conf_d, int conf0,
                   const cplx<R>* in, cplx<R>* out, const cplx<R>* U)
@@ -238,18 +258,16 @@ void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* co
     else if (variant == 5 && c->L.Nx % 32 == 0)
     {
         const dim3 grid(c->L.Nx / 32, (c->L.Nt + 7) / 8, nrhs);
-        if (dag)
-            dirac_colx_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
-        else
-            dirac_colx_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        auto kern = dag ? dirac_colx_kernel<true, R> : dirac_colx_kernel<false, R>;
+        prefer_l1(c, 0 + (dag ? 1 : 0) + (sizeof(R) == 8 ? 2 : 0), kern);
+        kern<<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
     }
     else if (variant == 1 || variant == 5)
     {
         const dim3 grid((c->L.Nx + 31) / 32, (c->L.Nt + 7) / 8, nrhs);
-        if (dag)
-            dirac_col_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
-        else
-            dirac_col_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        auto kern = dag ? dirac_col_kernel<true, R> : dirac_col_kernel<false, R>;
+        prefer_l1(c, 4 + (dag ? 1 : 0) + (sizeof(R) == 8 ? 2 : 0), kern);
+        kern<<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
     }
     else
     {
@@ -258,17 +276,19 @@ void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* co
                            ? std::min(nb, std::max(1, DWFB_DIRAC_BLOCKS_PER_SM * c->nsm))
                            : nb;
         const dim3 grid(bx, nrhs);
+        const int b = (dag ? 1 : 0) + (sizeof(R) == 8 ? 2 : 0);
         if (variant == 2 && c->L.Nx % 32 == 0)
         {
-            if (dag)
-                dirac_warp_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
-            else
-                dirac_warp_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+            auto kern = dag ? dirac_warp_kernel<true, R> : dirac_warp_kernel<false, R>;
+            prefer_l1(c, 8 + b, kern);
+            kern<<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
         }
-        else if (dag)
-            dirac_kernel<true, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
         else
-            dirac_kernel<false, R><<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        {
+            auto kern = dag ? dirac_kernel<true, R> : dirac_kernel<false, R>;
+            prefer_l1(c, 12 + b, kern);
+            kern<<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
+        }
     }
     c->launches += 1;
 }

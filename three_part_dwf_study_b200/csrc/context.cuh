@@ -35,6 +35,7 @@ struct dwf_ctx
     int dslash_variant = -1;
     int dslash_chunk = 0;    // rows per chunk of the t-sweeping Dslash (0 = automatic)
     int sweep_smem_set = 0;  // t-sweeping kernels whose shared-memory limit is raised (bits)
+    int l1_pref_set = 0;     // shared-memory-free Dslash kernels asked for the largest L1 (bits)
     std::map<int, DslashChoice> dslash_tuned;
     // CUDA events bracketing each persistent solver launch on `stream`
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -534,7 +534,8 @@ def wilson_dslash(T, local, dev, peak):
         tsec = e0.elapsed_time(e1) * 1e-3 / 20
         gbs = Nt * Nx * (2 * 4 * wb + 2 * 2 * wb) / tsec / 1e9
         out[f"complex{2 * prec}"] = {"GBs": round(gbs, 1), "frac": round(gbs / peak, 4),
-                                     "us_per_apply": round(tsec * 1e6, 2)}
+                                     "us_per_apply": round(tsec * 1e6, 2),
+                                     "kernel_variant": w.dslash_variant(prec, 1)}
     w.close()
     return out
 
@@ -727,7 +728,8 @@ def impl_ours(args):
         tsec = e0.elapsed_time(e1) * 1e-3 / reps
         gbs = dslash_bytes(Dt * Dx, Dl, w) / tsec / 1e9
         dslash[f"complex{2 * prec}"] = {"GBs": round(gbs, 1), "frac": round(gbs / peak, 4),
-                                         "us_per_apply": round(tsec * 1e6, 2)}
+                                         "us_per_apply": round(tsec * 1e6, 2),
+                                         "kernel_variant": dd.dslash_variant(prec, 1)}
     dslash["lattice"] = list(DSLASH_LATTICE)
     dslash["bytes_rule"] = "V*(Ls*64+32) B (FP64), V*(Ls*32+16) B (FP32) per application"
     dd.close()

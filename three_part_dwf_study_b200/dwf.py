@@ -337,6 +337,11 @@ class DomainWall(LearnedMixin):
         return dict(cpp=cpp, cj5=cj5, loop=loop, mom_cpp=mom[:, :nmom],
                     info=[i.as_dict() for i in infos])
 
+    def dslash_variant(self, precision, nrhs):
+        """The Dslash kernel the autotuner chose for a precision (64 or 32) and
+        batch size (-1 before the first application of that kind)."""
+        return int(A.lib().dwf_dslash_variant(self._h, int(precision), int(nrhs)))
+
     def launch_count(self):
         return int(A.lib().dwf_launch_count(self._h))
 

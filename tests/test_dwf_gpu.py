@@ -272,7 +272,7 @@ def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
     rng = np.random.default_rng(Nt + Nx)
     w = tdwf.Wilson(Nt, Nx, -0.3, 0.0, bc_t=-1.0, bc_x=-1.0)
     o = O.Wilson(Nt, Nx, -0.3, -1.0, -1.0)
-    assert A.lib().dwf_set_dslash_variant(w.handle, variant) == 0
+    w.set_dslash_variant(variant)
     th = random_theta(rng, Nt, Nx)
     psi = random_field(rng, 2 * o.ntot)
     for op, name in OPS:
@@ -282,7 +282,9 @@ def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
         y32 = torch.empty_like(x32)
         w.apply_dev(op, x32, y32)
         assert rel(y32.cpu().numpy(), ref) < 2e-6, name
-    assert A.lib().dwf_dslash_variant(w.handle, 32, 2) == variant
+    assert w.dslash_variant(32, 2) == variant
+    with pytest.raises(A.DwfError):
+        w.set_dslash_variant(6)
 
 
 def test_wilson_dslash_autotuned_matches_oracle(tdwf):

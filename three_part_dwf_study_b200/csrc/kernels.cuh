@@ -24,9 +24,10 @@ __global__ void dirac_warp_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>
 
 // Same operator, one thread per 4-D site sweeping s like dirac_col_kernel,
 // with the x neighbours and the backward x link exchanged by warp shuffles
-// (Nx % 32 == 0; the two edge lanes load theirs) and slice s+1's spinor loads
-// issued before slice s is computed (grid: Nx/32 x ceil(Nt/8) x nrhs, 256
-// threads, one t row per warp).
+// (Nx % 32 == 0; the two edge lanes load theirs), slice s+1's spinor loads
+// issued before slice s is computed and slice s+DWFB_COLX_PREFETCH prefetched
+// into L1 (grid: Nx/32 x ceil(Nt/8) x nrhs, 256 threads, one t row per warp;
+// launched with the largest-L1 shared-memory split preferred).
 template <bool DAG, typename R>
 __global__ void dirac_colx_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
                                   long fsz, const cplx<R>* __restrict__ U, long usz,

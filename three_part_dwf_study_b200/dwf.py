@@ -337,6 +337,15 @@ class DomainWall(LearnedMixin):
         return dict(cpp=cpp, cj5=cj5, loop=loop, mom_cpp=mom[:, :nmom],
                     info=[i.as_dict() for i in infos])
 
+    def set_dslash_variant(self, variant, chunk=None):
+        """Force a Dslash kernel for apply/apply_dev (0 site, 1 column, 2 site
+        with shuffled x neighbours, 3 t sweep, 4 Wilson rows, 5 column with
+        shuffled x neighbours; -1 autotune, the default), and optionally the t
+        sweep's chunk length in rows (0: automatic and tuned)."""
+        self._check(A.lib().dwf_set_dslash_variant(self._h, int(variant)))
+        if chunk is not None:
+            self._check(A.lib().dwf_set_dslash_chunk(self._h, int(chunk)))
+
     def dslash_variant(self, precision, nrhs):
         """The Dslash kernel the autotuner chose for a precision (64 or 32) and
         batch size (-1 before the first application of that kind)."""

@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(256)
                          [&](int s, const Spinor<R>& o) { st_spinor(outj, long(s) * L.V + here, o); });
 }
 
-// Slices of lookahead that dirac_colx_kernel prefetches into L1 (0: none).
+// Slices of lookahead that dirac_colx_kernel prefetches into L1 (0: none; at
+// 512x512x16, 1 / 2 / 3 slices gave 3794 / 4188 / 4108 GB/s in FP64).
 #ifndef DWFB_COLX_PREFETCH
 #define DWFB_COLX_PREFETCH 2
 #endif

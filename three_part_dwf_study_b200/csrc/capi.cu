@@ -333,6 +333,9 @@ DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, co
                         cand.push_back({3, tc, g});
         }
     }
+    // an error already pending belongs to the caller: tune only from a clean state
+    if (cudaPeekAtLastError() != cudaSuccess)
+        return cand.front();
     float best = 1e30f;
     DslashChoice choice = cand.front();
     for (const DslashChoice& ch : cand)
@@ -345,6 +348,9 @@ DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, co
         cudaEventSynchronize(c->ev1);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        // a candidate that failed to launch did no work: drop it rather than time it
+        if (cudaGetLastError() != cudaSuccess)
+            continue;
         if (ms < best)
         {
             best = ms;

@@ -318,15 +318,22 @@ int dwf_z4_digits(uint64_t seed, long n, signed char* out);
  * side, needing no context and calling no cudaMalloc, cudaFree or allocating
  * library routine. The caller passes device pointers it owns: theta_dev
  * (2*Nt*Nx angles), b_dev and x_dev (Ls*Nt*Nx*2 complex<double>; x read as the
- * guess when has_guess), and a cudaStream_t (or NULL) as void*. All other
+ * guess when has_guess), and a cudaStream_t as void* (NULL: the calling
+ * thread's per-thread default stream, never the legacy NULL stream). The call
+ * returns when the solve is done (it reads its report back). All other
  * buffers live in one static device array that each GPU loading the library
  * holds until exit: lattices up to DWF_NOALLOC_MAX_SITES = Ls*Nt*Nx sites and
  * DWF_NOALLOC_MAX_LINKS = 2*Nt*Nx links; larger ones return DWF_BAD_ARG.
  * params->device selects (and leaves current) the GPU. The first call on a
- * device resolves the array's device address, so make that first call before
- * any stream capture. Calls share the array: calls whose GPU work overlaps
- * race and must be serialised by the caller. Returns the solve status; info
- * (host, may be NULL) as dwf_cg reports it. */
+ * device resolves the array's device address (kept for the process's life,
+ * so no use across a cudaDeviceReset), so make that first call before any
+ * stream capture. While another thread holds a capture open, that capture
+ * must use cudaStreamCaptureModeThreadLocal or ...Relaxed: in global mode
+ * CUDA forbids every other thread the synchronous read-back this call makes.
+ * Calls share the array: calls whose GPU work overlaps race and must be
+ * serialised by the caller. Returns the solve status, or DWF_TIMEOUT when a
+ * wait inside the solver ran out; info (host, may be NULL) as dwf_cg reports
+ * it, also on DWF_TIMEOUT. */
 #define DWF_NOALLOC_MAX_SITES 65536
 #define DWF_NOALLOC_MAX_LINKS 32768
 int dwf_cg_noalloc(const dwf_params* params, int op, const double* theta_dev, const void* b_dev,

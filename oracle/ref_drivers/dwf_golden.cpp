@@ -1,6 +1,6 @@
 // Golden-vector driver for the domain-wall path (TEST INFRASTRUCTURE).
 // Compiled against the UNMODIFIED reference headers (domain_wall/include) and
-// the project-written Eigen-API subset in oracle/eigen_shim. Reads seeded
+// the project-written Eigen-API subset in three_part_dwf_study_b200/host/eigen_shim. Reads seeded
 // inputs written by tests/golden/make_golden.py from the working directory
 // (which also holds the parameters.txt the reference reads at start-up) and
 // writes full-precision outputs of the reference entry points:

@@ -1,7 +1,7 @@
 // Golden-vector driver for the Wilson path (TEST INFRASTRUCTURE).
 // Compiled against the UNMODIFIED reference headers (wilson/include, plus the
 // .npy reader/writer from domain_wall/include/npy_io.hpp) and the project-written
-// Eigen-API subset in oracle/eigen_shim. Writes full-precision outputs of:
+// Eigen-API subset in three_part_dwf_study_b200/host/eigen_shim. Writes full-precision outputs of:
 //   build_wilson_matrix (wilson_operator.hpp:10-62) applied as D psi and D^dag psi
 //   solve_CGNR, solve_DDdag (cg_solver.hpp:19-78)
 //   gauge_action_force, pseudofermion_action_force, average_plaquette (gauge.hpp:20-122)

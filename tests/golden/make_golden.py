@@ -3,15 +3,15 @@
 
 Runs in the build container only (it needs the reference sources): builds the
 reference's own C++ (domain_wall/*.cpp, wilson/*.cpp and the driver programs in
-oracle/ref_drivers, all compiled unmodified against oracle/eigen_shim) with
-``make -C oracle ref``, then for each case writes a parameters.txt and seeded
+oracle/ref_drivers, all compiled unmodified against the Eigen-API subset in
+three_part_dwf_study_b200/host/eigen_shim) with ``make -C oracle ref REF=<checkout>``, then for each case writes a parameters.txt and seeded
 inputs into a scratch directory, runs the reference there and copies the
 outputs into tests/golden/<case>/.
 
 Inputs are seeded synthetic fields: link phases uniform in [-pi, pi) and
 complex Gaussian spinors, as the lattice study's hot starts and heatbaths use.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference checkout>
 """
 import json
 import shutil
@@ -87,7 +87,9 @@ def run(cmd, cwd):
 
 
 def main():
-    subprocess.run(["make", "-C", str(REPO / "oracle"), "ref"], check=True)
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout>")
+    subprocess.run(["make", "-C", str(REPO / "oracle"), "ref", f"REF={sys.argv[1]}"], check=True)
     for name, (kind, over, seed) in CASES.items():
         params = dict(BASE)
         params.update(over)

@@ -75,3 +75,24 @@ def test_dropin_wilson_generate_and_analyze(golden, tmp_path, solver):
     run("analyze_wilson", tmp_path, solver)
     a, b = table(out / "correlators_by_config.csv"), table(g.dir / "correlators_by_config.csv")
     assert a.shape == b.shape and np.allclose(a, b, rtol=2e-5)
+
+
+@pytest.mark.parametrize("solver", ["cg64", "mixed"])
+def test_dropin_conjugate_gradient_forms(golden, tmp_path, solver):
+    """The drop-in conjugate_gradient in both forms (tests/dropin_src/cg_forms.cpp):
+    the named normal operator, the reference's std::function signature
+    (domain_wall/include/cg_solver.hpp:17-22) holding a b200::NormalOperator
+    (the same GPU solve: identical iterations and solution) and holding the
+    caller's own lambda over apply_D_dagger_D (host recurrences around the GPU
+    operator: same solution to CG accuracy)."""
+    g = golden("dwf_8x8x4")
+    shutil.copy2(g.dir / "parameters.txt", tmp_path / "parameters.txt")
+    out = run("cg_forms", tmp_path, solver)
+    rows = {ln.split()[0]: ln.split()[1:] for ln in out.strip().splitlines()}
+    assert set(rows) == {"named", "normal_operator", "lambda"}
+    for name, (it, conv, rr, dx) in rows.items():
+        assert int(conv) == 1 and float(rr) <= 1e-12, name
+    assert rows["normal_operator"][0] == rows["named"][0]
+    assert float(rows["normal_operator"][3]) == 0.0
+    assert abs(int(rows["lambda"][0]) - int(rows["named"][0])) <= 3 or solver != "cg64"
+    assert float(rows["lambda"][3]) < 1e-9

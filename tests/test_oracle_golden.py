@@ -177,3 +177,32 @@ def test_oracle_adjointness_and_free_field():
         v = np.round(np.asarray(v), 9)
         return v[np.lexsort((v.imag, v.real))]
     assert np.allclose(canon(ev), canon(expect), atol=1e-8)
+
+
+@pytest.mark.parametrize("case", DWF_CASES + WIL_CASES)
+def test_oracle_cg_at_1e14_is_the_exact_solution(golden, case):
+    """At rtol 1e-14 the oracle's CG (the reference algorithm) is within 1e-13
+    of a dense direct solve of the same normal equation, so GPU-against-oracle
+    comparisons at that tolerance measure rounding, not CG truncation: the
+    basis of the 1e-12 parity bar on FP64 solutions and forces."""
+    g = golden(case)
+    p = g.p
+    th = g.npy("in_theta.npy")
+    if case.startswith("dwf"):
+        o = dwf_of(g)
+        n = o.ndof
+        rhs = o.apply(O.D, th, g.field("in_chi.npy"))
+        eta = o.pf_action_force(th, rhs, 1e-14, 20000)["eta"]
+    else:
+        o = O.Wilson(p["wilson.Nt"], p["wilson.Nx"], p["wilson.m0"],
+                     p["wilson.time_boundary_sign"], p["wilson.space_boundary_sign"])
+        n = o.ntot
+        rhs = g.field("in_psi.npy")
+        st, eta, _ = o.solve_dddag(th, rhs, 1e-14, 20000)
+        assert st == 0
+        st, x, _ = o.solve_cgnr(th, rhs, 1e-14, 20000)
+        assert st == 0
+    Dm = np.array([o.apply(0, th, e) for e in np.eye(n)]).T
+    assert rel(eta, np.linalg.solve(Dm @ Dm.conj().T, rhs)) < 1e-13
+    if case.startswith("wil"):
+        assert rel(x, np.linalg.solve(Dm.conj().T @ Dm, Dm.conj().T @ rhs)) < 1e-13

@@ -337,6 +337,7 @@ DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, co
     if (cudaPeekAtLastError() != cudaSuccess)
         return cand.front();
     float best = 1e30f;
+    bool any = false;
     DslashChoice choice = cand.front();
     for (const DslashChoice& ch : cand)
     {
@@ -350,14 +351,24 @@ DslashChoice pick_variant(dwf_ctx* c, int nrhs, const int* conf_d, int conf0, co
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         // a candidate that failed to launch did no work: drop it rather than time it
         if (cudaGetLastError() != cudaSuccess)
+        {
+            // an error that reading does not clear is sticky: the context is
+            // lost, so stop launching into it
+            if (cudaPeekAtLastError() != cudaSuccess)
+                break;
             continue;
+        }
+        any = true;
         if (ms < best)
         {
             best = ms;
             choice = ch;
         }
     }
-    c->dslash_tuned[key] = choice;
+    // cache only a choice that ran; with none, the caller's own launch reports
+    // the error and the next call tunes again
+    if (any)
+        c->dslash_tuned[key] = choice;
     return choice;
 }
 

@@ -55,7 +55,10 @@ std::mutex g_mu;
 void* g_base[kMaxDevices] = {};
 
 // Device address of g_scratch on `dev` (must be current). In host code the
-// name g_scratch is only a host-side stand-in, never a device address.
+// name g_scratch is only a host-side stand-in, never a device address. The
+// address is resolved on the first call per device and kept for the life of
+// the process: a cudaDeviceReset of that device (which unloads the module)
+// leaves it stale, so the entry point must not be used across a device reset.
 int scratch_base(int dev, unsigned char** base)
 {
     if (dev < 0 || dev >= kMaxDevices)
@@ -91,7 +94,12 @@ extern "C" int dwf_cg_noalloc(const dwf_params* p, int op, const double* theta_d
     int st = scratch_base(p->device, &base);
     if (st)
         return st;
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    // NULL selects the calling thread's per-thread default stream, never the
+    // legacy NULL stream: work on the legacy stream would implicitly
+    // synchronise with (and so invalidate) a capture that another thread holds
+    // open on a blocking stream.
+    cudaStream_t stream =
+        stream_ptr ? static_cast<cudaStream_t>(stream_ptr) : cudaStreamPerThread;
     int nsm = 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess)
         return DWF_CUDA_ERROR;
@@ -199,13 +207,13 @@ extern "C" int dwf_cg_noalloc(const dwf_params* p, int op, const double* theta_d
         cudaMemcpyAsync(&hb, bar, sizeof(hb), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
         return DWF_CUDA_ERROR;
-    if (hb.err != 0)
-        return hb.err;
+    // a barrier error (a wait that ran out) outranks the solver's own status
+    const int status = hb.err != 0 ? hb.err : hi[1];
     if (info)
     {
         info->iterations = hi[0];
-        info->status = hi[1];
-        info->converged = hi[1] == DWF_OK ? 1 : 0;
+        info->status = status;
+        info->converged = status == DWF_OK ? 1 : 0;
         info->solver = DWF_SOLVER_CG64;
         info->relres = hd[0];
         info->true_relres = hd[1];
@@ -214,5 +222,5 @@ extern "C" int dwf_cg_noalloc(const dwf_params* p, int op, const double* theta_d
         info->dirac_relres = 0.0;
         info->schur_iterations = 0;
     }
-    return hi[1];
+    return status;
 }

@@ -7,7 +7,9 @@ configuration is built in the axial gauge from such plaquettes and then
 gauge-randomised. These serve as thermalised-like starting points of
 measurement ensembles and as the training configurations of the learned
 preconditioner; the dynamical-fermion HMC (DomainWall.hmc_trajectory) refines
-them where the fermion determinant matters.
+them where the fermion determinant matters. hmc_chain runs the reference
+generator's whole Markov chain (draws, leapfrog, Metropolis, thermalisation cut
+and thinning) on the GPU and yields HMC-generated ensembles.
 """
 import numpy as np
 
@@ -32,3 +34,44 @@ def quenched_ensemble(seed, n, Nt, Nx, beta):
     """n configurations [n][2 Nt Nx] from one seeded generator."""
     rng = np.random.default_rng(seed)
     return np.stack([quenched_theta(rng, Nt, Nx, beta) for _ in range(n)])
+
+
+def hmc_chain(d, theta0, trajectories, seed, epsilon, steps, rtol=1e-10, maxiter=5000,
+              solver=None, thermalization_cut=0, thin=1):
+    """The domain-wall generator's Markov chain on the GPU
+    (domain_wall/generate_configs.cpp:48-207): per trajectory, from one
+    std::mt19937_64(seed) stream, chi (Ndof complex, imaginary part first),
+    then the momenta (2 Nt Nx normals), then the Metropolis uniform; phi = D chi,
+    leapfrog (DomainWall.hmc_trajectory), accept if u < min(exp(-dH), 1).
+    Configurations from trajectory `thermalization_cut` on, every `thin`-th,
+    are kept (the reference's analysis_configs).
+
+    d: DomainWall context. Returns (configs [n][2 Nt Nx], history) with history
+    a dict of per-trajectory arrays accepted, dH, acceptance_probability,
+    plaquette (of the chain's configuration after the decision)."""
+    from . import _capi as A
+    from .rng import Rng
+
+    solver = A.SOLVER_MIXED if solver is None else solver
+    rng = Rng(seed)
+    th = np.ascontiguousarray(theta0, dtype=np.float64).reshape(-1).copy()
+    kept = []
+    hist = {k: np.zeros(trajectories) for k in ("accepted", "dH", "acceptance_probability",
+                                                 "plaquette")}
+    for k in range(trajectories):
+        chi = rng.pseudofermion(d.Ndof)
+        mom = rng.normals(d.Ngauge)
+        prop, info = d.hmc_trajectory(th, chi, mom, epsilon, steps, rtol=rtol, maxiter=maxiter,
+                                      solver=solver)
+        pacc = min(float(np.exp(-info["dH"])), 1.0)
+        acc = rng.uniform() < pacc
+        if acc:
+            th = prop
+        hist["accepted"][k] = acc
+        hist["dH"][k] = info["dH"]
+        hist["acceptance_probability"][k] = pacc
+        hist["plaquette"][k] = d.average_plaquette(th)
+        if k >= thermalization_cut and (k - thermalization_cut) % thin == 0:
+            kept.append(th.copy())
+    configs = np.stack(kept) if kept else np.zeros((0, d.Ngauge))
+    return configs, hist

@@ -1,7 +1,10 @@
 // Project-written stand-in for the small part of the Eigen 3 API that the
-// lattice study's C++ sources use. TEST INFRASTRUCTURE ONLY: it exists so the
-// unmodified reference headers (domain_wall/include/*.hpp, wilson/include/*.hpp)
-// compile in a container that has no Eigen installation. Nothing here is
+// lattice study's C++ sources use. It exists so that, on a host without an
+// Eigen installation, the unmodified reference headers (domain_wall/include/
+// *.hpp, wilson/include/*.hpp) compile for the CPU oracle and the reference's
+// mains compile against the drop-in headers (the drop-in build uses a system
+// Eigen 3 instead wherever one is installed). The GPU hot path does not use it:
+// there it only carries the host-side vector types across the C ABI. Nothing here is
 // Eigen source; every operation is written from its mathematical definition:
 //
 //   dense  : column vectors / small matrices of std::complex<double>, eager

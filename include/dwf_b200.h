@@ -379,6 +379,17 @@ int dwf_set_dslash_chunk(dwf_ctx* ctx, int rows);
 int dwf_eo_phase_profile(dwf_ctx* ctx, int enable);
 int dwf_eo_phase_times(dwf_ctx* ctx, double* ms, uint64_t* counts);
 
+/* ---- device selection ------------------------------------------------------------ */
+/* No counterpart in the reference (its executables are CPU programs). Number of
+ * CUDA devices visible to this process (DWF_CUDA_ERROR and 0 when none). */
+int dwf_device_count(int* count);
+/* The next device in turn, modulo ndevices, among the processes of this host
+ * that share counter_path (a small text file holding the next index, updated
+ * under an exclusive flock): each call takes one index. The drop-in headers
+ * call it when DWF_B200_DEVICE=auto, so that the study driver's concurrent
+ * cases (scripts/run_three_part_study.py:166-169) run on different GPUs. */
+int dwf_round_robin_device(int ndevices, const char* counter_path, int* device);
+
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);
 /* Accumulated device time (ms) of the persistent solver launches of one kind

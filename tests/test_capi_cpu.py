@@ -96,3 +96,29 @@ def test_host_random_streams_match_reference_draws():
         assert np.array_equal(r.pseudofermion(ndof), chi[k])
         assert r.uniform() == u[k]
     assert np.array_equal(z4_digits(5, 1000), O.rng_z4(5, 1000))
+
+
+def _rr_worker(path, q):
+    import ctypes as C
+    from three_part_dwf_study_b200 import _capi as A
+    dev = C.c_int(-1)
+    st = A.lib().dwf_round_robin_device(4, str(path).encode(), C.byref(dev))
+    q.put((st, dev.value))
+
+
+def test_round_robin_device_hands_out_each_gpu_in_turn(tmp_path):
+    """DWF_B200_DEVICE=auto: concurrent processes (here 8, for 4 GPUs) take the
+    counter under a lock, so every device index is handed out exactly twice."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    path = tmp_path / "counter"
+    procs = [ctx.Process(target=_rr_worker, args=(path, q)) for _ in range(8)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(st == 0 for st, _ in got)
+    assert sorted(d for _, d in got) == [0, 0, 1, 1, 2, 2, 3, 3]
+    assert path.read_text().strip() == "8"

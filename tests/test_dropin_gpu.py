@@ -26,7 +26,8 @@ def run(name, cwd, solver):
     exe = BIN / name
     if not exe.exists():
         pytest.skip(f"{exe} not built (needs the reference sources at build time)")
-    env = dict(os.environ, DWF_B200_SOLVER=solver)
+    # DWF_B200_DEVICE=auto: the device is handed out in turn (one GPU here: 0)
+    env = dict(os.environ, DWF_B200_SOLVER=solver, DWF_B200_DEVICE="auto", TMPDIR=str(cwd))
     r = subprocess.run([str(exe)], cwd=cwd, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     return r.stdout

@@ -39,6 +39,29 @@ inline int prop_solver()
     return s;
 }
 
+// CUDA device of this process's contexts: DWF_B200_DEVICE=<n> names one;
+// DWF_B200_DEVICE=auto takes the next device in turn among the processes that
+// start with it on this host (dwf_round_robin_device on a counter file in
+// $TMPDIR or /tmp), so that concurrent study cases spread over the GPUs;
+// unset, device 0.
+inline int device()
+{
+    static const int d = [] {
+        const char* v = std::getenv("DWF_B200_DEVICE");
+        if (!v || !*v)
+            return 0;
+        if (std::strcmp(v, "auto") != 0)
+            return std::atoi(v);
+        int n = 0, dev = 0;
+        if (dwf_device_count(&n) != DWF_OK || n < 1)
+            return 0;
+        const char* tmp = std::getenv("TMPDIR");
+        const std::string path = std::string(tmp && *tmp ? tmp : "/tmp") + "/dwf_b200_device_counter";
+        return dwf_round_robin_device(n, path.c_str(), &dev) == DWF_OK ? dev : 0;
+    }();
+    return d;
+}
+
 inline void check(dwf_ctx* c, int st)
 {
     if (st == DWF_OK)

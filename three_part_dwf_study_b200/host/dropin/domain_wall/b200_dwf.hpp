@@ -13,7 +13,7 @@ inline dwf_ctx* b200_dwf_context()
         dwf_ctx* c = nullptr;
         Holder()
         {
-            const dwf_params p{Nt, Nx, N5, M5, mf, beta, 0};
+            const dwf_params p{Nt, Nx, N5, M5, mf, beta, b200::device()};
             b200::check(nullptr, dwf_ctx_create(&p, &c));
         }
         ~Holder() { dwf_ctx_destroy(c); }

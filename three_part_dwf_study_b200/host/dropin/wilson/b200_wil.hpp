@@ -13,7 +13,7 @@ inline dwf_ctx* b200_wil_context()
         dwf_ctx* c = nullptr;
         Holder()
         {
-            const wil_params p{Nt, Nx, m0, beta, time_boundary_sign, space_boundary_sign, 0};
+            const wil_params p{Nt, Nx, m0, beta, time_boundary_sign, space_boundary_sign, b200::device()};
             b200::check(nullptr, wil_ctx_create(&p, &c));
         }
         ~Holder() { dwf_ctx_destroy(c); }

@@ -23,9 +23,16 @@ def gather_outputs(local, nconf, world, rank, device=None):
     """All-gather {name: array [n_local, ...]} into {name: array [nconf, ...]}
     in configuration order. Blocks are padded to the largest shard for the
     collective and trimmed afterwards."""
+    sizes = [partition(nconf, world, r)[1] - partition(nconf, world, r)[0] for r in range(world)]
+    if world == 1:
+        # one rank holds the whole ensemble: no collective (and no process group) needed
+        for name in local:
+            if np.shape(local[name])[0] != nconf:
+                raise ValueError(f"gather_outputs: {name} has {np.shape(local[name])[0]} rows, "
+                                 f"rank owns {nconf}")
+        return {name: np.asarray(local[name]) for name in sorted(local)}
     import torch
     import torch.distributed as dist
-    sizes = [partition(nconf, world, r)[1] - partition(nconf, world, r)[0] for r in range(world)]
     cap = max(sizes) if sizes else 0
     out = {}
     for name in sorted(local):

@@ -164,8 +164,10 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
         const long cap = long(bps) * c->nsm;
         int grid = 0;
         choose_units(d.L.nsite, n, cap, &d.nch, &d.ch, &grid);
-        // 4-D even sites: enough units for every block, at least 32 sites each
-        e.nch4 = int(std::max<long>(1, std::min<long>(g.Vh / 32, (grid + n - 1) / n)));
+        // 4-D even sites: at most one unit per block, so the phase ends after one
+        // unit's time (a unit count just above the grid made a few blocks take
+        // two units while the rest waited at the barrier), at least 32 sites each
+        e.nch4 = int(std::max<long>(1, std::min<long>(g.Vh / 32, grid / n)));
         e.ch4 = (g.Vh + e.nch4 - 1) / e.nch4;
         e.nch4 = (g.Vh + e.ch4 - 1) / e.ch4;
         st = ensure_part(c, size_t(n) * d.nch * 2);

@@ -370,6 +370,15 @@ int dwf_dslash_variant(const dwf_ctx* ctx, int precision, int nrhs);
  * choices. */
 int dwf_set_dslash_chunk(dwf_ctx* ctx, int rows);
 
+/* Kernel of the even-odd Schur solve: -1 automatic (default): one thread-
+ * block cluster per right-hand side with its FP32 fields in the cluster's
+ * distributed shared memory wherever one right-hand side fits (Nt divisible by
+ * the cluster size 8 or 16, Ls/4 in {4, 6}, ~200 KB of fields per CTA) and
+ * the device can co-schedule such clusters, else the grid-wide persistent
+ * kernel; 0 the grid-wide kernel always. The environment variable
+ * DWF_B200_EO_KERNEL=grid makes 0 the default of every context. */
+int dwf_set_eo_kernel(dwf_ctx* ctx, int kernel);
+
 /* Per-phase device timers of the even-odd solver kernel (block 0's view, each
  * phase including the grid barrier that ends it): enable (1) allocates and
  * zeroes them, 0 frees them (off by default: no cost). dwf_eo_phase_times
@@ -393,7 +402,8 @@ int dwf_round_robin_device(int ndevices, const char* counter_path, int* device);
 /* Number of kernels this context has launched so far. */
 uint64_t dwf_launch_count(const dwf_ctx* ctx);
 /* Accumulated device time (ms) of the persistent solver launches of one kind
- * (0: full-lattice CG kernels, 1: the even-odd Schur kernel), measured with
+ * (0: full-lattice CG kernels, 1: the even-odd Schur solve, either kernel,
+ * 2: the even-odd cluster kernel alone), measured with
  * CUDA events on the context stream; *nlaunch (optional) = their count. */
 double dwf_solver_kernel_ms(const dwf_ctx* ctx, int kind, uint64_t* nlaunch);
 

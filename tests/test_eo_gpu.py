@@ -100,3 +100,34 @@ def test_eo_phase_timers(T):
     assert all(ms[k] > 0.0 for k in (0, 1, 3, 4))
     assert A.lib().dwf_eo_phase_profile(d.handle, 0) == 0
     d.close()
+
+
+@pytest.mark.parametrize("shape,nrhs", [((64, 64, 16), 6), ((64, 32, 16), 20), ((32, 16, 24), 3)])
+def test_cluster_kernel_matches_grid_kernel(T, shape, nrhs):
+    """The even-odd solve on one thread-block cluster per right-hand side (FP32
+    fields in distributed shared memory; cluster of 16 CTAs at 64x64x16, of 8 at
+    64x32x16, Ls = 24 with six slices per lane at 32x16x24) against the
+    grid-wide kernel on the same sources: both meet the FP64 true residual, the
+    solutions agree to the solvers' accuracy and the Schur iteration counts
+    agree closely (more right-hand sides than clusters at 64x32x16, so
+    clusters take several right-hand sides in turn)."""
+    Nt, Nx, Ls = shape
+    rng = np.random.default_rng(Nt * Nx + Ls)
+    d = T.DomainWall(Nt, Nx, Ls, 1.0, 0.05)
+    from three_part_dwf_study_b200.ensemble import quenched_theta
+    d.set_gauge(quenched_theta(rng, Nt, Nx, 3.0))
+    src = boundary_sources(rng, Nt, Nx, Ls, nrhs)
+    n0 = d.solver_kernel_ms(2)[1]
+    x_cl, info_cl = d.propagators(src, rtol=1e-10, maxiter=20000, solver=T.SOLVER_EO_MIXED)
+    assert d.solver_kernel_ms(2)[1] == n0 + 1  # the cluster kernel ran
+    d.set_eo_kernel(0)
+    x_gr, info_gr = d.propagators(src, rtol=1e-10, maxiter=20000, solver=T.SOLVER_EO_MIXED)
+    d.set_eo_kernel(-1)
+    for k in range(nrhs):
+        c, g = info_cl[k], info_gr[k]
+        assert c["converged"] and c["true_relres"] <= 1e-10, k
+        assert g["converged"] and g["true_relres"] <= 1e-10, k
+        assert c["schur_iterations"] > 0
+        assert abs(c["schur_iterations"] - g["schur_iterations"]) <= 0.1 * g["schur_iterations"] + 8
+        assert rel(x_cl[k], x_gr[k]) < 1e-7, k
+    d.close()

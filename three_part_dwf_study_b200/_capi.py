@@ -101,6 +101,7 @@ SIGNATURES = {
     "dwf_propagators_dev": (_I, [_P, _I, _P, _P, _P, _D, _I, _I, C.POINTER(SolveInfo)]),
     "dwf_launch_count": (C.c_uint64, [_P]),
     "dwf_device_count": (_I, [C.POINTER(_I)]),
+    "dwf_set_eo_kernel": (_I, [_P, _I]),
     "dwf_round_robin_device": (_I, [_I, C.c_char_p, C.POINTER(_I)]),
     "dwf_set_dslash_variant": (_I, [_P, _I]),
     "dwf_dslash_variant": (_I, [_P, _I, _I]),

@@ -1073,7 +1073,7 @@ int dwf_barrier_selftest(dwf_ctx* c, int missing_blocks, uint64_t limit_ns)
 
 double dwf_solver_kernel_ms(const dwf_ctx* c, int kind, uint64_t* nlaunch)
 {
-    if (!c || kind < 0 || kind > 1)
+    if (!c || kind < 0 || kind > 2)
         return 0.0;
     if (nlaunch)
         *nlaunch = c->solver_launches[kind];

@@ -39,8 +39,10 @@ struct dwf_ctx
     std::map<int, DslashChoice> dslash_tuned;
     // CUDA events bracketing each persistent solver launch on `stream`
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    double solver_ms[2] = {0.0, 0.0};  // device time of solver launches: full lattice, even-odd
-    uint64_t solver_launches[2] = {0, 0};
+    // device time of solver launches: full lattice, even-odd (either kernel),
+    // even-odd cluster kernel alone
+    double solver_ms[3] = {0.0, 0.0, 0.0};
+    uint64_t solver_launches[3] = {0, 0, 0};
 
     // gauge configurations
     int nconf = 0;
@@ -99,6 +101,7 @@ struct dwf_ctx
     float2* eo_y32 = nullptr;
     float2* eo_e32 = nullptr;
     unsigned long long* eo_phase = nullptr;  // per-phase timers (dwf_eo_phase_profile)
+    int eo_kernel = -1;  // even-odd solver kernel: -1 automatic, 0 grid-wide (dwf_set_eo_kernel)
 
     // HMC workspace (allocated on first use)
     double* h_mom = nullptr;    // [2V]

@@ -148,16 +148,6 @@ template __global__ void eo_combine_kernel<true>(Lat, EoGeo, const double2*, con
 
 // ---- persistent mixed-precision Schur CG ------------------------------------
 
-#ifndef DWFB_EO_PAIR
-#define DWFB_EO_PAIR 0  // 1: the FP32 5-D phases visit two sites per thread and step (loads overlapped)
-#endif
-
-// Result of the P4 update at one site: the new e and r.
-struct EoP4Out
-{
-    Spinor<float> e, r;
-};
-
 #ifndef DWFB_EO_MINB
 #define DWFB_EO_MINB 2  // resident 256-thread blocks per SM the register budget targets (2: no spills)
 #endif
@@ -219,20 +209,6 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
             return;
         phase_mark(e.phase_ns, 0, ph_t);
         // P2: t = M5 p - H_oe y, |t|^2
-#if DWFB_EO_PAIR
-        sweep_sites_pair(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, true,
-                         [&](int j, int i, long uo) {
-                             const int ss = i / g.Vh, h = i - ss * g.Vh;
-                             return eo_combine_site<false, float>(
-                                 NoLd<float>{}, false, FieldLd<float>{d.p32 + j * fh}, true,
-                                 FieldLd<float>{e.y32 + j * fh}, true, d.U32 + uo, d.L, g, ss, h,
-                                 kOdd);
-                         },
-                         [&](int j, int i, const Spinor<float>& v) {
-                             st_spinor(d.t32 + j * fh, i, v);
-                             return make_double2(spinor_norm2(v), 0.0);
-                         });
-#else
         sweep_sites(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, true,
                     [&](int j, int i, long uo) {
                         const int ss = i / g.Vh, h = i - ss * g.Vh;
@@ -243,7 +219,6 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                         st_spinor(d.t32 + j * fh, i, v);
                         return make_double2(spinor_norm2(v), 0.0);
                     });
-#endif
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
         phase_mark(e.phase_ns, 1, ph_t);
@@ -280,26 +255,6 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
             return;
         phase_mark(e.phase_ns, 3, ph_t);
         // P4: Ap = M5^dag t - H^dag_oe y; e += alpha p; r -= alpha Ap
-#if DWFB_EO_PAIR
-        sweep_sites_pair(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, true,
-                         [&](int j, int i, long uo) {
-                             const int ss = i / g.Vh, h = i - ss * g.Vh;
-                             const float a = float(s.al[j]);
-                             const Spinor<float> ap = eo_combine_site<true, float>(
-                                 NoLd<float>{}, false, FieldLd<float>{d.t32 + j * fh}, true,
-                                 FieldLd<float>{e.y32 + j * fh}, true, d.U32 + uo, d.L, g, ss, h,
-                                 kOdd);
-                             const Spinor<float> p = ld_spinor(d.p32 + j * fh, i);
-                             const Spinor<float> ee = ld_spinor(d.e32 + j * fh, i);
-                             const Spinor<float> r = ld_spinor(d.r32 + j * fh, i);
-                             return EoP4Out{axpy(a, p, ee), axpy(-a, ap, r)};
-                         },
-                         [&](int j, int i, const EoP4Out& o) {
-                             st_spinor(d.e32 + j * fh, i, o.e);
-                             st_spinor(d.r32 + j * fh, i, o.r);
-                             return make_double2(spinor_norm2(o.r), 0.0);
-                         });
-#else
         sweep_sites(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, true,
                     [&](int j, int i, long uo) {
                         const int ss = i / g.Vh, h = i - ss * g.Vh;
@@ -316,7 +271,6 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                         st_spinor(d.r32 + j * fh, i, rn);
                         return make_double2(spinor_norm2(rn), 0.0);
                     });
-#endif
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
         phase_mark(e.phase_ns, 4, ph_t);
@@ -418,18 +372,6 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
             break;
         phase_mark(e.phase_ns, 5, ph_t);
         // P5: p = r + beta p
-#if DWFB_EO_PAIR
-        sweep_sites_pair(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, false,
-                         [&](int j, int i, long) {
-                             const Spinor<float> p = ld_spinor(d.p32 + j * fh, i);
-                             const Spinor<float> r = ld_spinor(d.r32 + j * fh, i);
-                             return axpy(float(s.cf[j]), p, r);
-                         },
-                         [&](int j, int i, const Spinor<float>& v) {
-                             st_spinor(d.p32 + j * fh, i, v);
-                             return make_double2(0.0, 0.0);
-                         });
-#else
         sweep_sites(d, s.act, nact, nsite5, d.nch, d.ch, s.scratch, false,
                     [&](int j, int i, long uo) {
                         const Spinor<float> p = ld_spinor(d.p32 + j * fh, i);
@@ -437,7 +379,6 @@ __global__ void __launch_bounds__(256, DWFB_EO_MINB) cg_eo_mixed_kernel(EoDesc e
                         st_spinor(d.p32 + j * fh, i, axpy(float(s.cf[j]), p, r));
                         return make_double2(0.0, 0.0);
                     });
-#endif
         if (!grid_sync(d.bar, d.expected_blocks, d.timeout_ns))
             return;
         phase_mark(e.phase_ns, 6, ph_t);

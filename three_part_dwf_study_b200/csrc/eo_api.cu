@@ -1,5 +1,7 @@
 // Host side of the even-odd preconditioned propagator solve.
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "context.cuh"
@@ -30,6 +32,19 @@ __global__ void eo_combine_kernel(Lat L, EoGeo g, const double2* a, const double
                                   const double2* y, double2* out, const double2* U, long usz,
                                   const int* conf, long nrhs);
 __global__ void cg_eo_mixed_kernel(EoDesc e);
+int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched);
+
+// DWF_B200_EO_KERNEL=grid keeps every even-odd solve on the grid-wide kernel
+// (cg_eo_mixed_kernel); by default the cluster kernel (eo_cluster.cu) takes
+// the batches whose right-hand side fits a cluster's shared memory.
+bool eo_cluster_enabled()
+{
+    static const bool on = [] {
+        const char* v = std::getenv("DWF_B200_EO_KERNEL");
+        return !(v && std::strcmp(v, "grid") == 0);
+    }();
+    return on;
+}
 
 bool eo_eligible(const dwf_ctx* c)
 {
@@ -141,6 +156,40 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
         e.xn64 = c->eo_xn;
         e.phase_ns = c->eo_phase;
 
+        bool clustered = false;
+        if (c->eo_kernel != 0 && eo_cluster_enabled())
+        {
+            CK(cudaEventRecord(c->ev0, c->stream));
+            st = launch_eo_cluster(c, e, &clustered);
+            if (st != DWF_OK && st != DWF_BAD_ARG)
+                return st;
+        }
+        if (clustered)
+        {
+            CK(cudaEventRecord(c->ev1, c->stream));
+            c->launches += 1;
+            std::vector<int> it(n), r(n);
+            CK(cudaMemcpyAsync(it.data(), c->w_iters, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(r.data(), c->w_ru, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            c->solver_ms[1] += ms;
+            c->solver_launches[1] += 1;
+            c->solver_ms[2] += ms;
+            c->solver_launches[2] += 1;
+            for (int k = 0; k < n; ++k)
+            {
+                iters[k0 + k] = it[k];
+                ru[k0 + k] = r[k];
+            }
+            eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_x, c->eo_se, -1.0, c->eo_y, c->U64, usz, c->w_conf, n);
+            eo_unpack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_y, c->eo_x, x + k0 * fs, n);
+            CK(cudaGetLastError());
+            c->launches += 2;
+            continue;
+        }
+
         const void* fn = reinterpret_cast<const void*>(&cg_eo_mixed_kernel);
         // the FP32 hop + M5^-1 phases keep each thread's Ls slices in shared
         // memory when that costs no resident blocks (registers bound them)
@@ -226,6 +275,14 @@ int dwf_eo_phase_profile(dwf_ctx* c, int enable)
     }
     if (c->eo_phase)
         CK(cudaMemsetAsync(c->eo_phase, 0, 16 * sizeof(unsigned long long), c->stream));
+    return DWF_OK;
+}
+
+int dwf_set_eo_kernel(dwf_ctx* c, int kernel)
+{
+    if (!c || kernel < -1 || kernel > 0)
+        return DWF_BAD_ARG;
+    c->eo_kernel = kernel;
     return DWF_OK;
 }
 

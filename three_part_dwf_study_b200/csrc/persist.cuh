@@ -135,54 +135,6 @@ __device__ void sweep_sites(const SolveDesc& d, const int* act, int nact, int ns
     }
 }
 
-// As sweep_sites with two sites per thread and step: fc(j, i, uo) loads and
-// computes a site's result without storing it, fs(j, i, r) stores it and
-// returns the two partial-sum contributions. Both sites' results are formed
-// before either is stored, so no store separates the two sites' loads and
-// they are in flight together (a store between them would order them, since
-// the compiler cannot prove the fields distinct).
-template <typename FC, typename FS>
-__device__ void sweep_sites_pair(const SolveDesc& d, const int* act, int nact, int nsite, int nch,
-                                 int ch, double* scratch, bool keep, FC fc, FS fs)
-{
-    const int nunits = nact * nch;
-    const int B = blockDim.x;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x)
-    {
-        const int k = u / nch, c = u - k * nch, j = act[k];
-        const int beg = c * ch;
-        const int end = min(beg + ch, nsite);
-        const long uo = long(d.rhs_conf[j]) * d.usz;
-        double a0 = 0.0, a1 = 0.0;
-        int i = beg + threadIdx.x;
-        for (; i + B < end; i += 2 * B)
-        {
-            const auto r0 = fc(j, i, uo);
-            const auto r1 = fc(j, i + B, uo);
-            const double2 v0 = fs(j, i, r0);
-            const double2 v1 = fs(j, i + B, r1);
-            a0 += v0.x + v1.x;
-            a1 += v0.y + v1.y;
-        }
-        if (i < end)
-        {
-            const double2 v = fs(j, i, fc(j, i, uo));
-            a0 += v.x;
-            a1 += v.y;
-        }
-        if (keep)
-        {
-            a0 = block_sum(a0, scratch);
-            a1 = block_sum(a1, scratch);
-            if (threadIdx.x == 0)
-            {
-                d.part[(long(j) * nch + c) * 2] = a0;
-                d.part[(long(j) * nch + c) * 2 + 1] = a1;
-            }
-        }
-    }
-}
-
 // The full-lattice sweep (nsite = Ls*V, the launch's chunking).
 template <typename F>
 __device__ void sweep(const SolveDesc& d, const int* act, int nact, double* scratch, bool keep,

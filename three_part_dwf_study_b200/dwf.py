@@ -337,6 +337,10 @@ class DomainWall(LearnedMixin):
         return dict(cpp=cpp, cj5=cj5, loop=loop, mom_cpp=mom[:, :nmom],
                     info=[i.as_dict() for i in infos])
 
+    def set_eo_kernel(self, kernel):
+        """Even-odd solve kernel: -1 automatic (cluster kernel where it fits), 0 grid-wide."""
+        self._check(A.lib().dwf_set_eo_kernel(self._h, int(kernel)))
+
     def set_dslash_variant(self, variant, chunk=None):
         """Force a Dslash kernel for apply/apply_dev (0 site, 1 column, 2 site
         with shuffled x neighbours, 3 t sweep, 4 Wilson rows, 5 column with
@@ -356,7 +360,7 @@ class DomainWall(LearnedMixin):
 
     def solver_kernel_ms(self, kind=0):
         """(ms, launches) of the persistent solver kernels of one kind:
-        0 full lattice, 1 even-odd."""
+        0 full lattice, 1 even-odd (either kernel), 2 even-odd cluster kernel."""
         n = C.c_uint64()
         ms = A.lib().dwf_solver_kernel_ms(self._h, int(kind), C.byref(n))
         return ms, n.value

@@ -339,6 +339,90 @@ __device__ __forceinline__ void cl_sync_global()
 
 }  // namespace
 
+// A thread's 4-D site in one of the FP32 phases, fixed for the whole solve:
+// where its four hop neighbours sit (slice 0) in the other parity's field.
+// The t neighbours are in this CTA's part (slice stride R Nxh) or in a halo
+// buffer (slice stride Nxh); the x neighbours are always in the own part.
+struct ClNbr
+{
+    int tp, tm;          // offsets of the t+1, t-1 neighbours at slice 0
+    bool tp_own, tm_own;
+    int xp, xm;          // own-part offsets of the x+1, x-1 neighbours at slice 0
+};
+
+template <class S>
+__device__ __forceinline__ ClNbr cl_nbr(int tl, int x)
+{
+    ClNbr n;
+    n.tp_own = tl + 1 < S::R;
+    n.tp = n.tp_own ? (tl + 1) * S::Nxh + (x >> 1) : S::Ls * S::Nxh + (x >> 1);
+    n.tm_own = tl >= 1;
+    n.tm = n.tm_own ? (tl - 1) * S::Nxh + (x >> 1) : (x >> 1);
+    const int xp = (x + 1 == S::Nx) ? 0 : x + 1;
+    const int xm = (x == 0) ? S::Nx - 1 : x - 1;
+    n.xp = tl * S::Nxh + (xp >> 1);
+    n.xm = tl * S::Nxh + (xm >> 1);
+    return n;
+}
+
+// The four link phases of the hops from (t, x), FP32, boundary signs folded in
+// (exact: the signs are +-1).
+struct ClLinks
+{
+    float2 t, tm, x, xm;
+};
+
+__device__ __forceinline__ ClLinks cl_links(const float2* __restrict__ U, const Lat& L, int Nt, int Nx,
+                                            int t, int x)
+{
+    const int tm = (t == 0) ? Nt - 1 : t - 1;
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+    const float stp = (t == Nt - 1) ? float(L.bct) : 1.f;
+    const float stm = (t == 0) ? float(L.bct) : 1.f;
+    const float sxp = (x == Nx - 1) ? float(L.bcx) : 1.f;
+    const float sxm = (x == 0) ? float(L.bcx) : 1.f;
+    return {stp * U[t * Nx + x], stm * U[tm * Nx + x], sxp * U[L.V + t * Nx + x], sxm * U[L.V + t * Nx + xm]};
+}
+
+// Hop term at slice s from precomputed neighbours and links (cl_hop for the
+// FP32 phases): own = the other parity field's own part, halo = its halo buffer.
+template <bool DAG, class S>
+__device__ __forceinline__ Spinor<float> cl_hop_pre(const float4* own, const float4* halo, const ClNbr& n,
+                                                    const ClLinks& u, int s)
+{
+    const float4 a = n.tp_own ? own[n.tp + s * S::n4] : halo[n.tp + s * S::Nxh];
+    const float4 b = n.tm_own ? own[n.tm + s * S::n4] : halo[n.tm + s * S::Nxh];
+    const float4 c = own[n.xp + s * S::n4];
+    const float4 d = own[n.xm + s * S::n4];
+    float2 up, lo;
+    hop4<DAG, float>(f4s(a), f4s(b), f4s(c), f4s(d), u.t, u.tm, u.x, u.xm, 1.f, 1.f, 1.f, 1.f, up, lo);
+    return {-0.5f * up, -0.5f * lo};
+}
+
+// M5 (M5^dag when DAG) at slice s of the own 4-D site h of an odd field.
+template <bool DAG, class S>
+__device__ __forceinline__ Spinor<float> cl_m5_pre(const float4* f, const Lat& L, int s, int h)
+{
+    const Spinor<float> c = f4s(f[s * S::n4 + h]);
+    const float dg = float(L.diag);
+    Spinor<float> o{dg * c.s0, dg * c.s1};
+    const int sup = (s + 1 == S::Ls) ? 0 : s + 1;
+    const float cup = (s + 1 == S::Ls) ? float(L.mf) : -1.f;
+    const int sdn = (s == 0) ? S::Ls - 1 : s - 1;
+    const float cdn = (s == 0) ? float(L.mf) : -1.f;
+    if (!DAG)
+    {
+        o.s1 += cup * f4s(f[sup * S::n4 + h]).s1;
+        o.s0 += cdn * f4s(f[sdn * S::n4 + h]).s0;
+    }
+    else
+    {
+        o.s1 += cdn * f4s(f[sdn * S::n4 + h]).s1;
+        o.s0 += cup * f4s(f[sup * S::n4 + h]).s0;
+    }
+    return o;
+}
+
 // Phase timer of cluster 0, rank 0, thread 0 (only when a phase buffer is
 // given; the same slots as the grid-wide kernel's).
 __device__ __forceinline__ void cl_mark(unsigned long long* ph, int k, unsigned long long& t)
@@ -388,6 +472,22 @@ __global__ void __launch_bounds__(kClThreads, 1) cg_eo_cluster_kernel(EoDesc e, 
     const ClRows rowsA{HA, t0, (t0 + G.Nt - 1) % G.Nt}, rowsB{HB, t0, (t0 + G.Nt - 1) % G.Nt};
     const ClLd<S> P{Pf, &rowsA}, E{Ef, &rowsA}, Tl{Tf, &rowsA}, Y{Yf, &rowsB};
     const HaloPush<S> pushA = halo_to<S>(HA, G.CS, rank), pushB = halo_to<S>(HB, G.CS, rank);
+    // thread roles of the FP32 phases, fixed for the solve: in the 4-D phases
+    // lanes 4h .. 4h+3 take even 4-D site h (lane q: slices q L4 .. q L4 + L4 - 1);
+    // in the 5-D phases thread h + g n4 takes odd 4-D site h and the slices
+    // g, g + G4, ... (G4 = threads / n4 slice groups)
+    static_assert(4 * S::n4 <= kClThreads, "one 4-D site per lane group");
+    constexpr int G4 = kClThreads / S::n4;
+    const int eh = threadIdx.x >> 2;
+    const bool e_on = eh < S::n4;
+    const int etl = e_on ? eh / S::Nxh : 0, ek = e_on ? eh - etl * S::Nxh : 0;
+    const int et = t0 + etl, ex = 2 * ek + (et & 1);
+    const ClNbr enb = cl_nbr<S>(etl, ex);
+    const int oh = threadIdx.x % S::n4, og = threadIdx.x / S::n4;
+    const bool o_on = og < G4;
+    const int otl = oh / S::Nxh, ok = oh - otl * S::Nxh;
+    const int ot = t0 + otl, ox = 2 * ok + ((ot + 1) & 1);
+    const ClNbr onb = cl_nbr<S>(otl, ox);
     const long fh = d.fsz;  // complex entries of one global parity field
     const int q = threadIdx.x & 3;
 
@@ -400,6 +500,8 @@ __global__ void __launch_bounds__(kClThreads, 1) cg_eo_cluster_kernel(EoDesc e, 
         double2* xj = d.x + j * fh;
         double2* t64 = d.t + j * fh;
         double2* y64 = e.y64 + j * fh;
+        const ClLinks eu = cl_links(U32, L, G.Nt, S::Nx, et, ex);
+        const ClLinks ou = cl_links(U32, L, G.Nt, S::Nx, ot, ox);
         // ---- x = 0: r = b, r32 = p32 = r, e32 = 0; |b|^2 ----
         double a0 = 0.0;
         for (int l = threadIdx.x; l < S::n5; l += kClThreads)
@@ -426,43 +528,36 @@ __global__ void __launch_bounds__(kClThreads, 1) cg_eo_cluster_kernel(EoDesc e, 
         for (int it = 1; it <= d.maxiter && state == RHS_ACTIVE; ++it)
         {
             // P1: y = M5^-1 H_eo p (four lanes per even 4-D site)
-            for (int w = threadIdx.x; w < 4 * S::n4 + ((4 * S::n4) % 32 ? 32 - (4 * S::n4) % 32 : 0);
-                 w += kClThreads)
             {
-                const int h = w >> 2;
-                const bool on = h < S::n4;
-                const int tl = on ? h / S::Nxh : 0, k = on ? h - tl * S::Nxh : 0;
-                const int t = t0 + tl, x = 2 * k + (t & 1);
                 Spinor<float> z[L4];
 #pragma unroll
                 for (int jj = 0; jj < L4; ++jj)
-                    z[jj] = on ? cl_hop<false, float, S>(P, U32, L, G.Nt, q * L4 + jj, t, x) : Spinor<float>{};
+                    z[jj] = e_on ? cl_hop_pre<false, S>(Pf, HA, enb, eu, q * L4 + jj) : Spinor<float>{};
                 cl_m5inv<false, float, L4>(z, q, pw32, S::Ls, float(L.mf));
-                if (on)
+                if (e_on)
 #pragma unroll
                     for (int jj = 0; jj < L4; ++jj)
                     {
                         const float4 v = s2f4(z[jj]);
-                        Yf[((q * L4 + jj) * S::R + tl) * S::Nxh + k] = v;
-                        pushB.put(q * L4 + jj, tl, k, v);
+                        Yf[(q * L4 + jj) * S::n4 + eh] = v;
+                        pushB.put(q * L4 + jj, etl, ek, v);
                     }
             }
             cl_sync();
             cl_mark(e.phase_ns, 0, ph_t);
             // P2: t = M5 p - H_oe y, |t|^2
             a0 = 0.0;
-            for (int l = threadIdx.x; l < S::n5; l += kClThreads)
-            {
-                const int s = l / S::n4, rem = l - s * S::n4, tl = rem / S::Nxh, k = rem - tl * S::Nxh;
-                const int t = t0 + tl, x = 2 * k + ((t + 1) & 1);
-                const Spinor<float> m = cl_m5<false, float>(P, L, S::Ls, s, t, k);
-                const Spinor<float> hy = cl_hop<false, float, S>(Y, U32, L, G.Nt, s, t, x);
-                const Spinor<float> v{m.s0 - hy.s0, m.s1 - hy.s1};
-                const float4 v4 = s2f4(v);
-                Tf[l] = v4;
-                pushA.put(s, tl, k, v4);
-                a0 += spinor_norm2(v);
-            }
+            if (o_on)
+                for (int sl = og; sl < S::Ls; sl += G4)
+                {
+                    const Spinor<float> m = cl_m5_pre<false, S>(Pf, L, sl, oh);
+                    const Spinor<float> hy = cl_hop_pre<false, S>(Yf, HB, onb, ou, sl);
+                    const Spinor<float> v{m.s0 - hy.s0, m.s1 - hy.s1};
+                    const float4 v4 = s2f4(v);
+                    Tf[sl * S::n4 + oh] = v4;
+                    pushA.put(sl, otl, ok, v4);
+                    a0 += spinor_norm2(v);
+                }
             a0 = block_sum(a0, scratch);
             if (threadIdx.x == 0)
                 red[1] = a0;
@@ -478,46 +573,40 @@ __global__ void __launch_bounds__(kClThreads, 1) cg_eo_cluster_kernel(EoDesc e, 
             const float al = float(rr / tt);
             cl_mark(e.phase_ns, 2, ph_t);
             // P3: y = M5^dag^-1 H^dag_eo t
-            for (int w = threadIdx.x; w < 4 * S::n4 + ((4 * S::n4) % 32 ? 32 - (4 * S::n4) % 32 : 0);
-                 w += kClThreads)
             {
-                const int h = w >> 2;
-                const bool on = h < S::n4;
-                const int tl = on ? h / S::Nxh : 0, k = on ? h - tl * S::Nxh : 0;
-                const int t = t0 + tl, x = 2 * k + (t & 1);
                 Spinor<float> z[L4];
 #pragma unroll
                 for (int jj = 0; jj < L4; ++jj)
-                    z[jj] = on ? cl_hop<true, float, S>(Tl, U32, L, G.Nt, q * L4 + jj, t, x) : Spinor<float>{};
+                    z[jj] = e_on ? cl_hop_pre<true, S>(Tf, HA, enb, eu, q * L4 + jj) : Spinor<float>{};
                 cl_m5inv<true, float, L4>(z, q, pw32, S::Ls, float(L.mf));
-                if (on)
+                if (e_on)
 #pragma unroll
                     for (int jj = 0; jj < L4; ++jj)
                     {
                         const float4 v = s2f4(z[jj]);
-                        Yf[((q * L4 + jj) * S::R + tl) * S::Nxh + k] = v;
-                        pushB.put(q * L4 + jj, tl, k, v);
+                        Yf[(q * L4 + jj) * S::n4 + eh] = v;
+                        pushB.put(q * L4 + jj, etl, ek, v);
                     }
             }
             cl_sync();
             cl_mark(e.phase_ns, 3, ph_t);
             // P4: Ap = M5^dag t - H^dag_oe y; e += alpha p; r -= alpha Ap; |r|^2
             a0 = 0.0;
-            for (int l = threadIdx.x; l < S::n5; l += kClThreads)
-            {
-                const int s = l / S::n4, rem = l - s * S::n4, tl = rem / S::Nxh, k = rem - tl * S::Nxh;
-                const int t = t0 + tl, x = 2 * k + ((t + 1) & 1);
-                const Spinor<float> m = cl_m5<true, float>(Tl, L, S::Ls, s, t, k);
-                const Spinor<float> hy = cl_hop<true, float, S>(Y, U32, L, G.Nt, s, t, x);
-                const Spinor<float> ap{m.s0 - hy.s0, m.s1 - hy.s1};
-                const Spinor<float> p = f4s(Pf[l]);
-                const float4 en = s2f4(persist::axpy(al, p, f4s(Ef[l])));
-                Ef[l] = en;
-                pushA.put(s, tl, k, en);
-                const Spinor<float> rn = persist::axpy(-al, ap, f4s(Rf[l]));
-                Rf[l] = s2f4(rn);
-                a0 += spinor_norm2(rn);
-            }
+            if (o_on)
+                for (int sl = og; sl < S::Ls; sl += G4)
+                {
+                    const int l = sl * S::n4 + oh;
+                    const Spinor<float> m = cl_m5_pre<true, S>(Tf, L, sl, oh);
+                    const Spinor<float> hy = cl_hop_pre<true, S>(Yf, HB, onb, ou, sl);
+                    const Spinor<float> ap{m.s0 - hy.s0, m.s1 - hy.s1};
+                    const Spinor<float> p = f4s(Pf[l]);
+                    const float4 en = s2f4(persist::axpy(al, p, f4s(Ef[l])));
+                    Ef[l] = en;
+                    pushA.put(sl, otl, ok, en);
+                    const Spinor<float> rn = persist::axpy(-al, ap, f4s(Rf[l]));
+                    Rf[l] = s2f4(rn);
+                    a0 += spinor_norm2(rn);
+                }
             a0 = block_sum(a0, scratch);
             if (threadIdx.x == 0)
                 red[2] = a0;
@@ -622,13 +711,14 @@ __global__ void __launch_bounds__(kClThreads, 1) cg_eo_cluster_kernel(EoDesc e, 
             cl_mark(e.phase_ns, 5, ph_t);
             // P5: p = r + beta p
             const float beta = float(cf);
-            for (int l = threadIdx.x; l < S::n5; l += kClThreads)
-            {
-                const int s = l / S::n4, rem = l - s * S::n4, tl = rem / S::Nxh, k = rem - tl * S::Nxh;
-                const float4 v = s2f4(persist::axpy(beta, f4s(Pf[l]), f4s(Rf[l])));
-                Pf[l] = v;
-                pushA.put(s, tl, k, v);
-            }
+            if (o_on)
+                for (int sl = og; sl < S::Ls; sl += G4)
+                {
+                    const int l = sl * S::n4 + oh;
+                    const float4 v = s2f4(persist::axpy(beta, f4s(Pf[l]), f4s(Rf[l])));
+                    Pf[l] = v;
+                    pushA.put(sl, otl, ok, v);
+                }
             cl_sync();
             cl_mark(e.phase_ns, 6, ph_t);
         }

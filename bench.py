@@ -6,8 +6,8 @@ line names in `kernel_variant`).
 
 Workload (one "step"): the per-configuration propagator set of the
 domain-wall analyzer on a 64x64 lattice, Ls = 16, M5 = 1.0, m_f = 0.05 on a
-seeded beta = 3.0 gauge configuration (pure-gauge plaquette distribution,
-three_part_dwf_study_b200.ensemble): 2 spins x 4 source
+beta = 3.0 gauge configuration thermalised by the GPU HMC (one chain of the
+reference generator's loop, tests/golden/make_bench_configs.py): 2 spins x 4 source
 times boundary point sources, 16 complex Z4 boundary-noise sources and
 2 spins x 2 source times boundary wall sources (28 right-hand sides), each
 solved as x = (D^dag D)^-1 D^dag src (domain_wall/include/correlator.hpp
@@ -19,7 +19,7 @@ equation is <= 1e-10.
 One JSON line on rank 0. `value` = right-hand sides solved per second across
 all ranks by the fastest of the solvers measured (even-odd mixed CG, or the
 learned-preconditioned mixed BiCGStab, whose network is trained on four
-other configurations of the same ensemble; training time reported apart),
+other configurations of the same HMC chain; training time reported apart),
 inputs resident in HBM, CUDA-event device time, max over ranks;
 `e2e` = the same through the host C-ABI entry (dwf_set_gauge + dwf_propagators
 from pinned host buffers, solutions read back). With --gpus N (torchrun) every
@@ -58,14 +58,24 @@ DSLASH_LATTICE = (512, 512, 16)
 L2_FLUSH_BYTES = 256 << 20
 
 
+BENCH_CONFIGS = REPO / "tests" / "golden" / "bench_hmc_64x64x16" / "configs.npy"
+
+
+def bench_configs():
+    """Configurations of one GPU-HMC Markov chain at the workload's parameters
+    (tests/golden/make_bench_configs.py): 0-7 per-rank workloads, 8-11 the
+    learned preconditioner's training set."""
+    if not BENCH_CONFIGS.exists():
+        raise SystemExit(f"{BENCH_CONFIGS} is missing: run tests/golden/make_bench_configs.py on a GPU")
+    return np.load(BENCH_CONFIGS)
+
+
 def workload_gauge(rank):
-    from three_part_dwf_study_b200.ensemble import quenched_theta
-    return quenched_theta(np.random.default_rng(GAUGE_SEED + 7919 * rank), NT, NX, BETA)
+    return bench_configs()[rank % 8].copy()
 
 
 def training_gauges(rank):
-    from three_part_dwf_study_b200.ensemble import quenched_ensemble
-    return quenched_ensemble(GAUGE_SEED + 1000003 + 7919 * rank, 4, NT, NX, BETA)
+    return bench_configs()[8:12].copy()
 
 
 LP_HIDDEN = 32
@@ -474,6 +484,66 @@ def analysis_batches(T, local, nconf=8):
     return out
 
 
+def analysis_study(nconf=64, therm=10):
+    """The finite-volume scan's analysis at full size: for each Nx in {32, 56,
+    80, 96} (Nt = 64, Ls = 16, m_f = 0.05, beta = 3), nconf configurations of
+    one GPU-HMC chain (the reference generator's loop, leapfrog epsilon = 0.01
+    with 40 steps, mixed-CG pseudofermion solves to 1e-10, therm thermalisation
+    trajectories from a seeded pure-gauge start, every configuration after them
+    kept), then all their propagators -- 8 point, 16 Z4-noise and 4 wall sources
+    per configuration, nconf * 28 right-hand sides -- in one dwf_measure call
+    (one batched even-odd solve to 1e-10 plus every contraction), and the
+    analyzer's reductions on the host. One JSON line: per Nx the HMC time and
+    acceptance, the measurement's device time (CUDA events on the library
+    stream, host copies included), solves/s, Schur iterations, plaquette and
+    m_res."""
+    import torch
+    import three_part_dwf_study_b200 as T
+    from three_part_dwf_study_b200 import analysis
+    from three_part_dwf_study_b200.ensemble import hmc_chain, quenched_theta
+    from three_part_dwf_study_b200.rng import z4_digits
+    out = {"configurations_per_Nx": nconf, "rhs_per_configuration": 28, "rtol": RTOL}
+    for Nx in (32, 56, 80, 96):
+        Nt, Ls = 64, 16
+        d = T.DomainWall(Nt, Nx, Ls, M5, MF, BETA)
+        th0 = quenched_theta(np.random.default_rng(GAUGE_SEED + Nx), Nt, Nx, BETA)
+        t0 = time.perf_counter()
+        cfg, hist = hmc_chain(d, th0, therm + nconf, seed=GAUGE_SEED + 17 * Nx, epsilon=HMC_EPS,
+                              steps=HMC_STEPS, rtol=RTOL, maxiter=MAXITER, solver=T.SOLVER_MIXED,
+                              thermalization_cut=therm)
+        hmc_s = time.perf_counter() - t0
+        z4 = np.concatenate([z4_digits(NOISE_SEED + 104729 * k, N_NOISE * Nt * Nx * 2)
+                             for k in range(nconf)])
+        kw = dict(z4=z4, n_point_times=4, n_wall_times=2, n_noise=N_NOISE, max_momentum=5,
+                  rtol=RTOL, maxiter=MAXITER, solver=T.SOLVER_EO_MIXED)
+        st = torch.cuda.ExternalStream(d.stream_ptr())
+        n_cl = d.solver_kernel_ms(2)[1]
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        m = d.measure(cfg, **kw)
+        e1.record(st)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3
+        if not all(i["converged"] for i in m["info"]):
+            raise SystemExit(f"analysis study: a solve did not converge (Nx={Nx})")
+        red = analysis.reduce_ensemble(m, Nt, Nx, 2)
+        nr = len(m["info"])
+        out[f"64x{Nx}x16"] = {
+            "hmc_seconds": sig(hmc_s), "hmc_trajectories": therm + nconf,
+            "acceptance": sig(float(hist["accepted"].mean())),
+            "plaquette_mean": sig(float(hist["plaquette"][therm:].mean())),
+            "rhs": nr, "measure_seconds": sig(sec), "solves_per_s": sig(nr / sec),
+            "ms_per_configuration": sig(1e3 * sec / nconf),
+            "schur_iterations_mean": sig(statistics.mean(i["schur_iterations"] for i in m["info"])),
+            "eo_kernel": "cluster" if d.solver_kernel_ms(2)[1] > n_cl else "grid",
+            "m_res": sig(red["m_res_average"])}
+        d.close()
+    print(json.dumps({"analysis_study": out}))
+    return 0
+
+
 # DWF 128x128, Ls = 24, M5 = 1, m_f = 0.02, beta = 4: the larger HMC comparison
 C5_LATTICE, C5_M5, C5_MF, C5_BETA = (128, 128, 24), 1.0, 0.02, 4.0
 
@@ -585,8 +655,8 @@ def wilson_dslash(T, local, dev, peak):
 
 def workload_config(solver):
     return {
-        "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, seeded beta=3.0 "
-                     f"start, 28 boundary sources per step (8 point, 16 Z4 noise, 4 wall), "
+        "workload": (f"DWF propagator solves, {NT}x{NX} Ls={LS} M5={M5} mf={MF}, GPU-HMC beta=3.0 "
+                     f"configuration, 28 boundary sources per step (8 point, 16 Z4 noise, 4 wall), "
                      f"to FP64 true residual {RTOL:g} of D^dag D"),
         "lattice": [NT, NX, LS], "rhs_per_step": 28, "rtol": RTOL, "solver": solver,
         "l2": "flushed between steps (256 MiB write)",
@@ -623,6 +693,7 @@ def impl_ours(args):
         torch.cuda.synchronize(dev)
 
     def timed(fn, steps, warmup, kind):
+        # kind 1 is the even-odd solve (either kernel); kind 2 counts the cluster kernel alone
         for _ in range(warmup):
             fn()
         barrier()
@@ -786,6 +857,8 @@ def impl_ours(args):
     wil = wilson_learned_grid(T) if (args.wilson_learned and ws == 1) else None
 
     # ---- roofline of the dominant kernel (the persistent even-odd solver) ----
+    eo_kernel_name = ("cg_eo_cluster_kernel (one thread-block cluster per right-hand side)"
+                      if d.solver_kernel_ms(2)[1] > 0 else "cg_eo_mixed_kernel")
     V = NT * NX
     iters = sum(i["schur_iterations"] for infos in infos_m for i in infos)
     rus = sum(i["reliable_updates"] for infos in infos_m for i in infos)
@@ -798,7 +871,7 @@ def impl_ours(args):
         traffic = json.loads(tfile.read_text()).get("cg_eo_mixed_kernel_bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "cg_eo_mixed_kernel", "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+                "kernel": eo_kernel_name, "peak_kind": f"{peak_kind} hbm_gbs (burst)",
                 "alg_bytes_per_launch": alg_bytes / max(1, nkern),
                 "kernel_ms_per_launch": kernel_launch_s * 1e3,
                 "kernel_share_of_step": kern_s / t_mixed}
@@ -825,7 +898,7 @@ def impl_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": ("bf16 network + f32 BiCGStab + f64 defect correction" if use_learned else
                   "f32+f64 (FP32 inner CG, FP64 reliable updates and true residual)"),
-        "data": "synthetic (seeded beta=3.0 pure-gauge configuration, boundary point/Z4/wall sources)",
+        "data": "synthetic (beta=3.0 configuration thermalised by the GPU HMC, boundary point/Z4/wall sources)",
         "config": dict(workload_config(
             "learned-preconditioned mixed BiCGStab (FP64 defect correction)" if use_learned else
             "even-odd Schur mixed FP32/FP64 CG, then the full D^dag D check"),
@@ -1102,6 +1175,8 @@ def main():
     ap.add_argument("--profile-wilson-dslash", action="store_true")
     ap.add_argument("--dslash-variants", action="store_true")
     ap.add_argument("--eo-phases", action="store_true")
+    ap.add_argument("--analysis-study", action="store_true",
+                    help="64 GPU-HMC configurations per Nx in {32,56,80,96}, all propagators in one call")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case()
@@ -1117,6 +1192,8 @@ def main():
         return dslash_variants()
     if args.eo_phases:
         return eo_phases()
+    if args.analysis_study:
+        return analysis_study()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

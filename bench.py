@@ -868,7 +868,9 @@ def impl_ours(args):
     traffic = None
     tfile = REPO / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("cg_eo_mixed_kernel_bytes_per_launch")
+        traffic = json.loads(tfile.read_text()).get(
+            "cg_eo_cluster_kernel_bytes_per_launch" if eo_kernel_name.startswith("cg_eo_cluster")
+            else "cg_eo_mixed_kernel_bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "kernel": eo_kernel_name, "peak_kind": f"{peak_kind} hbm_gbs (burst)",

@@ -78,8 +78,8 @@ typedef enum
     DWF_SOLVER_EO_MIXED = 2,
     /* Propagator solves with the learned preconditioner (no counterpart in the
      * reference; needs dwf_lp_init, normally followed by dwf_lp_train): FP64
-     * defect correction around an FP32 BiCGStab on D x = src, right-
-     * preconditioned by the gauge-equivariant network N ~ D^-1 (BF16 channel
+     * defect correction around an FP32 flexible GCR (dwf_lp_set_krylov) on
+     * D x = src, right-preconditioned by the gauge-equivariant network N ~ D^-1 (BF16 channel
      * mixing, FP32 accumulation); the reference's stopping rule
      * |D^dag (D x - src)| <= rtol |D^dag src| is checked on the FP64 true
      * residual after each inner solve. A right-hand side whose true residual
@@ -476,6 +476,20 @@ int dwf_lp_set_variant(dwf_ctx* ctx, int variant);
 /* Inner solve: stop at |r| <= inner_tol |r0| or inner_maxiter iterations;
  * at most outer_max defect-correction cycles (defaults 3e-4, 400, 40). */
 int dwf_lp_set_solver(dwf_ctx* ctx, double inner_tol, int inner_maxiter, int outer_max);
+/* Inner Krylov method of DWF_SOLVER_LEARNED: DWF_LP_GCR (default) is flexible
+ * GCR restarted every `restart` iterations (4, 8, 12 or 16; default 4), one
+ * network application and one D per iteration: z_k = N r, w_k = D z_k
+ * orthogonalised against the cycle's earlier w (classical Gram-Schmidt), the
+ * minimal-residual step on r, and the cycle's correction formed from the
+ * stored z_k, so N need not be the same operator in every iteration.
+ * DWF_LP_BICGSTAB is right-preconditioned BiCGStab (two network applications
+ * and two D per iteration; restart ignored). */
+enum
+{
+    DWF_LP_GCR = 0,
+    DWF_LP_BICGSTAB = 1
+};
+int dwf_lp_set_krylov(dwf_ctx* ctx, int method, int restart);
 
 
 #ifdef __cplusplus

@@ -215,9 +215,38 @@ def test_trained_network_beats_untrained_and_plain_cg(T):
     it_un = sum(i["schur_iterations"] + (i["iterations"] - i["schur_iterations"]) for i in un)
     it_cg = sum(i["iterations"] for i in cg)
     assert all(i["converged"] for i in tr + un + cg)
-    # D applications: learned 2 per BiCGStab iteration, CG 2 per iteration
+    # D applications: learned 1 per GCR iteration, CG 2 per iteration
     assert it_tr < 0.7 * it_un
-    assert 2 * it_tr < 0.5 * 2 * it_cg
+    assert it_tr < 0.5 * 2 * it_cg
+    d.close()
+
+
+@pytest.mark.parametrize("method,restart", [(0, 4), (0, 8), (0, 16), (1, 8)])
+def test_learned_krylov_methods_meet_rule(T, method, restart):
+    """Flexible GCR at each restart length and BiCGStab: every right-hand
+    side meets the stopping rule on the FP64 true residual without the
+    fallback and equals the FP64 solution."""
+    d, th, untrained, tinfo = learned_setup(T, 16, 16, 8, 3.0, 16, 600)
+    src = point_sources(16, 16, 8, 6)
+    conf = np.arange(6, dtype=np.int32) % 4
+    x64, _ = d.propagators(src, rhs_conf=conf, rtol=1e-12, maxiter=40000, solver=T.SOLVER_CG64)
+    d.lp_set_krylov(method, restart)
+    x, info = d.propagators(src, rhs_conf=conf, rtol=1e-10, maxiter=20000, solver=T.SOLVER_LEARNED)
+    for k in range(6):
+        assert info[k]["converged"] and info[k]["true_relres"] <= 1e-10, info[k]
+        assert info[k]["fallback"] == 0 and info[k]["schur_iterations"] > 0
+        assert rel(x[k], x64[k]) < 1e-7
+    d.close()
+
+
+def test_learned_krylov_rejects_bad_restart(T):
+    d = T.DomainWall(8, 8, 4, 1.0, 0.1)
+    d.set_gauge(np.zeros(2 * 64))
+    d.lp_init(hidden=8, seed=1)
+    for method, restart in ((0, 6), (0, 20), (0, 0), (2, 8)):
+        with pytest.raises(T.DwfError):
+            d.lp_set_krylov(method, restart)
+    d.lp_set_krylov(1, 0)
     d.close()
 
 

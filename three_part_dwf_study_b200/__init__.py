@@ -6,10 +6,11 @@ compute entry point raises.
 """
 from . import _capi
 from ._capi import (OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD, SOLVER_CG64, SOLVER_MIXED, SOLVER_EO_MIXED, SOLVER_LEARNED,
-                    DwfError,
+                    LP_GCR, LP_BICGSTAB, DwfError,
                     LIB_PATH)
 from .dwf import DomainWall, CgResult
 from .wilson import Wilson
 
 __all__ = ["DomainWall", "Wilson", "CgResult", "DwfError", "OP_D", "OP_DDAG", "OP_DDDAG", "OP_DDAGD",
-           "SOLVER_CG64", "SOLVER_MIXED", "SOLVER_EO_MIXED", "SOLVER_LEARNED", "LIB_PATH"]
+           "SOLVER_CG64", "SOLVER_MIXED", "SOLVER_EO_MIXED", "SOLVER_LEARNED", "LP_GCR", "LP_BICGSTAB",
+           "LIB_PATH"]

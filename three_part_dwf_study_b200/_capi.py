@@ -15,6 +15,7 @@ DWF_OK, DWF_NOT_CONVERGED, DWF_ZERO_DENOM, DWF_NONFINITE = 0, 1, 2, 3
 DWF_CUDA_ERROR, DWF_TIMEOUT, DWF_BAD_ARG = 4, 5, 6
 OP_D, OP_DDAG, OP_DDDAG, OP_DDAGD = 0, 1, 2, 3
 SOLVER_CG64, SOLVER_MIXED, SOLVER_EO_MIXED, SOLVER_LEARNED = 0, 1, 2, 3
+LP_GCR, LP_BICGSTAB = 0, 1
 
 
 class DwfParams(C.Structure):
@@ -140,6 +141,7 @@ SIGNATURES = {
     "dwf_lp_loss_grad_dev": (_I, [_P, _I, _P, _P, _P, C.POINTER(C.c_double), _P]),
     "dwf_lp_train": (_I, [_P, C.POINTER(LpTrainParams), C.POINTER(LpTrainInfo), _P]),
     "dwf_lp_set_solver": (_I, [_P, _D, _I, _I]),
+    "dwf_lp_set_krylov": (_I, [_P, _I, _I]),
     "dwf_lp_set_variant": (_I, [_P, _I]),
     "dwf_lp_time_network": (_I, [_P, _I, _I, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }

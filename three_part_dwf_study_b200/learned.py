@@ -132,3 +132,8 @@ class LearnedMixin:
     def lp_set_solver(self, inner_tol=3e-4, inner_maxiter=400, outer_max=40):
         self._check(A.lib().dwf_lp_set_solver(self._h, float(inner_tol), int(inner_maxiter),
                                               int(outer_max)))
+
+    def lp_set_krylov(self, method=A.LP_GCR, restart=4):
+        """Inner Krylov method of the learned solver: LP_GCR (flexible GCR
+        restarted every `restart` iterations, 4/8/12/16) or LP_BICGSTAB."""
+        self._check(A.lib().dwf_lp_set_krylov(self._h, int(method), int(restart)))

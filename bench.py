@@ -1105,6 +1105,83 @@ def eo_phases():
     return 0
 
 
+REF_GENERATE = REPO / "oracle" / "_ref" / "generate_domain_wall"
+REF_ANALYZE = REPO / "oracle" / "_ref" / "analyze_domain_wall"
+
+
+def ref_hmc_trajectory():
+    """B4: one reference HMC trajectory (domain_wall/generate_configs.cpp,
+    unmodified, one thread as the reference's generator runs) on the bench
+    lattice (64x64, Ls = 16, m_f = 0.05, beta = 3, epsilon = 0.01, 40 leapfrog
+    steps, pseudofermion CG to 1e-10), from the generator's own seeded start;
+    wall time of the process."""
+    with tempfile.TemporaryDirectory() as tmp:
+        d = Path(tmp)
+        (d / "output" / "domain_wall").mkdir(parents=True)
+        t = ref_params_text(MAXITER).replace("dwf.leapfrog_steps = 1",
+                                             f"dwf.leapfrog_steps = {HMC_STEPS}")
+        (d / "parameters.txt").write_text(t)
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        t0 = time.perf_counter()
+        r = subprocess.run([str(REF_GENERATE)], cwd=d, env=env, capture_output=True, text=True,
+                           timeout=7200)
+        sec = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise SystemExit(f"reference generator failed: {r.stderr.strip()[-400:]}")
+    return {"seconds_per_trajectory": round(sec, 2), "threads": 1, "lattice": [NT, NX, LS],
+            "epsilon": HMC_EPS, "leapfrog_steps": HMC_STEPS, "rtol": RTOL,
+            "source": "domain_wall/generate_configs.cpp, one trajectory"}
+
+
+def ref_analyzer(Nx=32, noise=8, nconf=None):
+    """B6: the reference analyzer (domain_wall/analyze_configs.cpp, unmodified)
+    on Nt = 64, Nx, Ls = 16 for nconf seeded beta = 3 configurations (default:
+    as many as host threads; the first ones are the bench's `analysis_batched`
+    configurations), analysis.threads = 0 (one configuration per OpenMP
+    thread), propagators to 1e-10, eta.noise_vectors = noise (8, the value in
+    the reference's parameters.txt): per configuration 2 x 2 wall, 2 x 2 point
+    and `noise` noise solves plus the contractions; seconds per configuration =
+    wall time / configurations."""
+    from three_part_dwf_study_b200.ensemble import quenched_theta
+    nconf = nconf or (os.cpu_count() or 1)
+    with tempfile.TemporaryDirectory() as tmp:
+        d = Path(tmp)
+        (d / "output" / "domain_wall").mkdir(parents=True)
+        Nt, Ls = 64, 16
+        t = ref_params_text(MAXITER, Nt, Nx, Ls).replace(
+            "eta.noise_vectors = 1", f"eta.noise_vectors = {noise}").replace(
+            "analysis.max_momentum = 1", "analysis.max_momentum = 5")
+        (d / "parameters.txt").write_text(t)
+        rng = np.random.default_rng(GAUGE_SEED + Nx)
+        th = np.stack([quenched_theta(rng, Nt, Nx, BETA).reshape(2, Nt, Nx) for _ in range(nconf)])
+        np.save(d / "output" / "domain_wall" / "analysis_configs.npy", th)
+        t0 = time.perf_counter()
+        r = subprocess.run([str(REF_ANALYZE)], cwd=d, capture_output=True, text=True, timeout=7200)
+        sec = time.perf_counter() - t0
+    measured = r.stdout.count("measuring config")
+    if measured != nconf:
+        raise SystemExit(f"reference analyzer measured {measured} of {nconf} configurations: "
+                         f"{r.stderr.strip()[-400:]}")
+    rhs = 4 + 4 + noise
+    return {"seconds_per_configuration": round(sec / nconf, 3), "configurations": nconf,
+            "threads": os.cpu_count() or 1, "wall_seconds": round(sec, 2),
+            "rhs_per_configuration": rhs, "solves_per_s": round(rhs * nconf / sec, 3),
+            "lattice": [Nt, Nx, Ls], "rtol": RTOL, "exit_code": r.returncode,
+            "source": "domain_wall/analyze_configs.cpp, all configurations in one run"}
+
+
+def cpu_reference_extras():
+    """BASELINE's B4 (reference HMC trajectory) and B6 (reference analyzer per
+    configuration) on the host cores, one JSON line (their GPU counterparts:
+    the bench line's `hmc_64x64x16` and `analysis_batched`)."""
+    if not (REF_GENERATE.exists() and REF_ANALYZE.exists()):
+        print(json.dumps({"cpu_reference_extras": "unavailable: oracle/_ref executables not built"}))
+        return 0
+    out = {"B6_analyzer_64x32x16": ref_analyzer(32), "B4_hmc_trajectory_64x64x16": ref_hmc_trajectory()}
+    print(json.dumps({"cpu_reference_extras": out}))
+    return 0
+
+
 def dslash_variants():
     """Event-timed GB/s of the Dslash kernels (site, column, site with shuffled
     x neighbours, t sweep at the automatic and at fixed chunk lengths, and for
@@ -1180,7 +1257,11 @@ def main():
     ap.add_argument("--eo-phases", action="store_true")
     ap.add_argument("--analysis-study", action="store_true",
                     help="64 GPU-HMC configurations per Nx in {32,56,80,96}, all propagators in one call")
+    ap.add_argument("--cpu-reference-extras", action="store_true",
+                    help="time the reference's own HMC trajectory (B4) and analyzer (B6) on the host cores")
     args = ap.parse_args()
+    if args.cpu_reference_extras:
+        return cpu_reference_extras()
     if args.profile_case:
         return profile_case()
     if args.profile_dslash:

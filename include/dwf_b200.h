@@ -406,6 +406,13 @@ uint64_t dwf_launch_count(const dwf_ctx* ctx);
  * 2: the even-odd cluster kernel alone), measured with
  * CUDA events on the context stream; *nlaunch (optional) = their count. */
 double dwf_solver_kernel_ms(const dwf_ctx* ctx, int kind, uint64_t* nlaunch);
+/* Even-odd propagator solves on the cluster kernel (dwf_propagators,
+ * dwf_measure and their device forms; no counterpart in the reference) run
+ * each chunk's source preparation, solver launch and reconstruction as one
+ * CUDA graph, captured on the first call and replayed while the chunk's size,
+ * buffers and settings repeat (the 16 most recent are kept per context).
+ * Returns the number of replays so far; *cached (optional) = graphs held. */
+uint64_t dwf_graph_replays(const dwf_ctx* ctx, int* cached);
 
 /* ---- learned preconditioner (no counterpart in the reference) ------------------ */
 /* A gauge-equivariant parallel-transport convolution network N ~ D^-1 of four

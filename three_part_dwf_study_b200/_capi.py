@@ -129,6 +129,7 @@ SIGNATURES = {
     "wil_solve_dddag": (_I, [_P, _P, _P, _D, _I, _I, _P, _P]),
     "wil_hmc_step": (_I, [_P, C.POINTER(HmcParams), _P, _P, _P, _D, _P, C.POINTER(TrajInfo)]),
     "dwf_solver_kernel_ms": (C.c_double, [_P, _I, C.POINTER(C.c_uint64)]),
+    "dwf_graph_replays": (C.c_uint64, [_P, C.POINTER(C.c_int)]),
     "dwf_eo_phase_profile": (_I, [_P, _I]),
     "dwf_eo_phase_times": (_I, [_P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "dwf_lp_init": (_I, [_P, _I, C.c_uint64]),

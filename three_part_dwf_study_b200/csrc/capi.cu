@@ -863,6 +863,9 @@ int dwf_ctx_destroy(dwf_ctx* c)
     for (void* b : bufs)
         if (b)
             cudaFree(b);
+    for (auto& g : c->graphs)
+        if (g.exec)
+            cudaGraphExecDestroy(g.exec);
     if (c->ev0)
         cudaEventDestroy(c->ev0);
     if (c->ev1)
@@ -1118,6 +1121,15 @@ double dwf_solver_kernel_ms(const dwf_ctx* c, int kind, uint64_t* nlaunch)
     if (nlaunch)
         *nlaunch = c->solver_launches[kind];
     return c->solver_ms[kind];
+}
+
+uint64_t dwf_graph_replays(const dwf_ctx* c, int* cached)
+{
+    if (!c)
+        return 0;
+    if (cached)
+        *cached = int(c->graphs.size());
+    return c->graph_replays;
 }
 
 }  // extern "C"

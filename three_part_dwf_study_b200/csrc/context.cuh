@@ -102,6 +102,17 @@ struct dwf_ctx
     float2* eo_e32 = nullptr;
     unsigned long long* eo_phase = nullptr;  // per-phase timers (dwf_eo_phase_profile)
     int eo_kernel = -1;  // even-odd solver kernel: -1 automatic, 0 grid-wide (dwf_set_eo_kernel)
+    // captured even-odd propagator chunks (source preparation, the cluster
+    // solver launch, reconstruction), most recent last, replayed when the
+    // chunk's size, buffers and settings repeat
+    struct GraphEntry
+    {
+        std::vector<uintptr_t> key;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+    };
+    std::vector<GraphEntry> graphs;
+    uint64_t graph_replays = 0;
 
     // HMC workspace (allocated on first use)
     double* h_mom = nullptr;    // [2V]

@@ -1,5 +1,6 @@
 // Host side of the even-odd preconditioned propagator solve.
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -32,7 +33,7 @@ __global__ void eo_combine_kernel(Lat L, EoGeo g, const double2* a, const double
                                   const double2* y, double2* out, const double2* U, long usz,
                                   const int* conf, long nrhs);
 __global__ void cg_eo_mixed_kernel(EoDesc e);
-int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched);
+int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched, bool dry);
 
 // DWF_B200_EO_KERNEL=grid keeps every even-odd solve on the grid-wide kernel
 // (cg_eo_mixed_kernel); by default the cluster kernel (eo_cluster.cu) takes
@@ -86,6 +87,56 @@ int ensure_eo(dwf_ctx* c, int nrhs)
     return DWF_OK;
 }
 
+constexpr size_t kGraphCache = 16;
+
+// Run `body` (stream work only) through a CUDA graph cached under `key`:
+// replay it if present, else capture it on the context stream (thread-local
+// mode) and launch the instantiated graph. If capture or instantiation fails,
+// `body` runs again directly. The cache keeps the kGraphCache most recent
+// graphs.
+template <typename F>
+int run_graph(dwf_ctx* c, const std::vector<uintptr_t>& key, F body)
+{
+    for (size_t i = 0; i < c->graphs.size(); ++i)
+        if (c->graphs[i].key == key)
+        {
+            dwf_ctx::GraphEntry g = c->graphs[i];
+            c->graphs.erase(c->graphs.begin() + long(i));
+            c->graphs.push_back(g);
+            CK(cudaGraphLaunch(g.exec, c->stream));
+            c->launches += g.launches;
+            c->graph_replays += 1;
+            return DWF_OK;
+        }
+    // errors pending from earlier calls are the caller's; capture only from a clean state
+    if (cudaPeekAtLastError() != cudaSuccess)
+        return body();
+    const uint64_t l0 = c->launches;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (st == DWF_OK && e == cudaSuccess && graph &&
+        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess)
+    {
+        cudaGraphDestroy(graph);
+        if (c->graphs.size() >= kGraphCache)
+        {
+            cudaGraphExecDestroy(c->graphs.front().exec);
+            c->graphs.erase(c->graphs.begin());
+        }
+        c->graphs.push_back({key, exec, c->launches - l0});
+        CK(cudaGraphLaunch(exec, c->stream));
+        return DWF_OK;
+    }
+    if (graph)
+        cudaGraphDestroy(graph);
+    cudaGetLastError();
+    c->launches = l0;
+    return body();
+}
+
 }  // namespace
 
 int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
@@ -111,15 +162,26 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
         CK(cudaMemcpyAsync(c->w_conf, conf.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
         const int nb = std::max(1, 8 * c->nsm);
         const long usz = c->usz();
-        // b_e, b_o; bhat = b_o - H_oe M5^-1 b_e; rhs = Dhat^dag bhat
-        eo_pack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, src + k0 * fs, c->eo_se, c->eo_so, n);
-        eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, nullptr, c->eo_se, 1.0, c->eo_y, c->U64, usz, c->w_conf, n);
-        eo_combine_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_so, nullptr, c->eo_y, c->eo_bh, c->U64, usz, c->w_conf, n);
-        eo_hopinv_kernel<true><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_bh, nullptr, 1.0, c->eo_y, c->U64, usz, c->w_conf, n);
-        eo_combine_kernel<true><<<nb, 256, 0, c->stream>>>(c->L, g, nullptr, c->eo_bh, c->eo_y, c->eo_rhs_o, c->U64, usz, c->w_conf, n);
-        CK(cudaGetLastError());
-        c->launches += 5;
-        CK(cudaMemsetAsync(c->eo_x, 0, size_t(n) * fh * sizeof(double2), c->stream));
+        // b_e, b_o; bhat = b_o - H_oe M5^-1 b_e; rhs = Dhat^dag bhat; x_o = 0
+        auto prepare = [&]() -> int {
+            eo_pack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, src + k0 * fs, c->eo_se, c->eo_so, n);
+            eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, nullptr, c->eo_se, 1.0, c->eo_y, c->U64, usz, c->w_conf, n);
+            eo_combine_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_so, nullptr, c->eo_y, c->eo_bh, c->U64, usz, c->w_conf, n);
+            eo_hopinv_kernel<true><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_bh, nullptr, 1.0, c->eo_y, c->U64, usz, c->w_conf, n);
+            eo_combine_kernel<true><<<nb, 256, 0, c->stream>>>(c->L, g, nullptr, c->eo_bh, c->eo_y, c->eo_rhs_o, c->U64, usz, c->w_conf, n);
+            CK(cudaGetLastError());
+            c->launches += 5;
+            CK(cudaMemsetAsync(c->eo_x, 0, size_t(n) * fh * sizeof(double2), c->stream));
+            return DWF_OK;
+        };
+        // x_e = M5^-1 (b_e - H_eo x_o); x = (x_e, x_o)
+        auto reconstruct = [&]() -> int {
+            eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_x, c->eo_se, -1.0, c->eo_y, c->U64, usz, c->w_conf, n);
+            eo_unpack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_y, c->eo_x, x + k0 * fs, n);
+            CK(cudaGetLastError());
+            c->launches += 2;
+            return DWF_OK;
+        };
 
         EoDesc e{};
         SolveDesc& d = e.d;
@@ -159,15 +221,39 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
         bool clustered = false;
         if (c->eo_kernel != 0 && eo_cluster_enabled())
         {
-            CK(cudaEventRecord(c->ev0, c->stream));
-            st = launch_eo_cluster(c, e, &clustered);
+            st = launch_eo_cluster(c, e, &clustered, true);
             if (st != DWF_OK && st != DWF_BAD_ARG)
                 return st;
         }
         if (clustered)
         {
-            CK(cudaEventRecord(c->ev1, c->stream));
-            c->launches += 1;
+            // preparation, the cluster solver and the reconstruction as one
+            // graph, replayed while the chunk's buffers and settings repeat
+            const std::vector<uintptr_t> key = {
+                uintptr_t(n), uintptr_t(src + k0 * fs), uintptr_t(x + k0 * fs), uintptr_t(c->w_conf),
+                uintptr_t(c->U64), uintptr_t(c->U32), uintptr_t(c->eo_se), uintptr_t(c->eo_so),
+                uintptr_t(c->eo_bh), uintptr_t(c->eo_rhs_o), uintptr_t(c->eo_x), uintptr_t(c->eo_r),
+                uintptr_t(c->eo_t), uintptr_t(c->eo_y), uintptr_t(c->eo_xn), uintptr_t(c->eo_r32),
+                uintptr_t(c->eo_p32), uintptr_t(c->eo_t32), uintptr_t(c->eo_y32), uintptr_t(c->eo_e32),
+                uintptr_t(c->w_iters), uintptr_t(c->w_relres), uintptr_t(c->w_status), uintptr_t(c->w_ru),
+                uintptr_t(c->eo_phase), uintptr_t(c->bar), uintptr_t(maxiter), uintptr_t(c->timeout_ns),
+                uintptr_t(std::llround(std::log2(tol) * 1e6)), uintptr_t(d.ru_period)};
+            st = run_graph(c, key, [&]() -> int {
+                int s2 = prepare();
+                if (s2)
+                    return s2;
+                // external records: event nodes of the graph, not capture markers
+                CK(cudaEventRecordWithFlags(c->ev0, c->stream, cudaEventRecordExternal));
+                bool l = false;
+                s2 = launch_eo_cluster(c, e, &l, false);
+                if (s2 || !l)
+                    return s2 ? s2 : ctx_fail(c, DWF_CUDA_ERROR, "even-odd cluster solver: launch failed");
+                CK(cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal));
+                c->launches += 1;
+                return reconstruct();
+            });
+            if (st)
+                return st;
             std::vector<int> it(n), r(n);
             CK(cudaMemcpyAsync(it.data(), c->w_iters, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaMemcpyAsync(r.data(), c->w_ru, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -183,12 +269,11 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
                 iters[k0 + k] = it[k];
                 ru[k0 + k] = r[k];
             }
-            eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_x, c->eo_se, -1.0, c->eo_y, c->U64, usz, c->w_conf, n);
-            eo_unpack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_y, c->eo_x, x + k0 * fs, n);
-            CK(cudaGetLastError());
-            c->launches += 2;
             continue;
         }
+        st = prepare();
+        if (st)
+            return st;
 
         const void* fn = reinterpret_cast<const void*>(&cg_eo_mixed_kernel);
         // the FP32 hop + M5^-1 phases keep each thread's Ls slices in shared
@@ -247,11 +332,9 @@ int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, 
             iters[k0 + k] = it[k];
             ru[k0 + k] = r[k];
         }
-        // x_e = M5^-1 (b_e - H_eo x_o); x = (x_e, x_o)
-        eo_hopinv_kernel<false><<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_x, c->eo_se, -1.0, c->eo_y, c->U64, usz, c->w_conf, n);
-        eo_unpack_kernel<<<nb, 256, 0, c->stream>>>(c->L, g, c->eo_y, c->eo_x, x + k0 * fs, n);
-        CK(cudaGetLastError());
-        c->launches += 2;
+        st = reconstruct();
+        if (st)
+            return st;
     }
     return DWF_OK;
 }

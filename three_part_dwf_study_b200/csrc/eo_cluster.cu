@@ -30,6 +30,8 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "context.cuh"
@@ -745,8 +747,20 @@ DWFB_CL_SHAPES(DWFB_CL_INST)
 // EoDesc as for cg_eo_mixed_kernel). Returns DWF_BAD_ARG (nothing launched)
 // when the lattice or the device does not allow it: the caller then runs the
 // grid-wide kernel.
-int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched)
+// Launch shape of the cluster kernel per (device, kernel): attributes set and
+// the resident-cluster count queried once, so that a later call (the one a
+// stream capture records) issues the launch alone.
+struct ClLaunchShape
 {
+    int nclust = 0;
+};
+
+// dry: check that the cluster kernel takes this batch and prepare its launch
+// shape without launching (*launched tells whether it would launch).
+int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched, bool dry)
+{
+    static std::map<std::pair<int, const void*>, ClLaunchShape> shapes;
+    static std::mutex shapes_mu;
     *launched = false;
     const Lat& L = c->L;
     const int Ls = L.Ls;
@@ -801,8 +815,11 @@ int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched)
 #undef DWFB_CL_PICK
     if (!fn)
         return DWF_BAD_ARG;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
-        (CS > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess))
+    std::lock_guard<std::mutex> lock(shapes_mu);
+    ClLaunchShape& sh = shapes[std::make_pair(c->device, fn)];
+    if (sh.nclust == 0 &&
+        (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
+         (CS > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)))
     {
         cudaGetLastError();
         return DWF_BAD_ARG;
@@ -819,13 +836,22 @@ int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cfg.gridDim = dim3(unsigned(CS * std::max(1, e.d.nrhs)));
-    int nclust = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclust, fn, &cfg) != cudaSuccess || nclust < 1)
+    if (sh.nclust == 0)
     {
-        cudaGetLastError();
-        return DWF_BAD_ARG;
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, fn, &cfg) != cudaSuccess || nc < 1)
+        {
+            cudaGetLastError();
+            return DWF_BAD_ARG;
+        }
+        sh.nclust = nc;
     }
-    nclust = std::min(nclust, e.d.nrhs);
+    if (dry)
+    {
+        *launched = true;
+        return DWF_OK;
+    }
+    const int nclust = std::min(sh.nclust, e.d.nrhs);
     cfg.gridDim = dim3(unsigned(CS * nclust));
     void* args[] = {&e, &cd};
     if (cudaLaunchKernelExC(&cfg, fn, args) != cudaSuccess)

@@ -365,6 +365,13 @@ class DomainWall(LearnedMixin):
         ms = A.lib().dwf_solver_kernel_ms(self._h, int(kind), C.byref(n))
         return ms, n.value
 
+    def graph_replays(self):
+        """(replays so far, graphs cached) of the captured even-odd propagator
+        chunks."""
+        n = C.c_int()
+        r = A.lib().dwf_graph_replays(self._h, C.byref(n))
+        return int(r), n.value
+
     def sync(self):
         self._check(A.lib().dwf_sync(self._h))
 

@@ -48,8 +48,6 @@ NT, NX, LS = 64, 64, 16
 M5, MF, BETA = 1.0, 0.05, 3.0
 RTOL = 1.0e-10
 MAXITER = 20000
-POINT_TIMES = (0, 16, 32, 48)
-WALL_TIMES = (0, 32)
 N_NOISE = 16
 GAUGE_SEED = 20260101
 NOISE_SEED = 918273
@@ -83,41 +81,43 @@ LP_TRAIN = dict(steps=4000, batch=8, lr=3e-3, lr_decay_steps=1333, pairs_per_con
                 solver_iters=50, solver_every=2, solver_maxiter=20000, seed=11)
 
 
-def fi(s, t, x, a):
-    return ((s * NT + t) * NX + x) * 2 + a
-
-
-def workload_sources(rank):
-    """28 boundary sources (complex128 [28, Ndof]). P_L = diag(0, 1),
-    P_R = diag(1, 0): spin 1 of the source sits on s = 0, spin 0 on s = Ls-1
-    (correlator.hpp:133-138, :201-211, :60-75)."""
-    ndof = LS * NT * NX * 2
+def boundary_source_set(Nt, Nx, Ls, seed):
+    """28 boundary sources (complex128 [28, Ndof]): 2 spins at 4 point-source
+    times (0, Nt/4, Nt/2, 3Nt/4), 16 Z4 noise vectors, 2 spins at 2 wall times
+    (0, Nt/2). P_L = diag(0, 1), P_R = diag(1, 0): spin 1 of the source sits on
+    s = 0, spin 0 on s = Ls-1 (correlator.hpp:133-138, :201-211, :60-75)."""
     srcs = []
-    for t in POINT_TIMES:
+    for t in (0, Nt // 4, Nt // 2, 3 * Nt // 4):
         for b in (0, 1):
-            v = np.zeros(ndof, np.complex128)
+            v = np.zeros((Ls, Nt, Nx, 2), np.complex128)
             if b == 1:
-                v[fi(0, t, 0, 1)] = 1.0
+                v[0, t, 0, 1] = 1.0
             else:
-                v[fi(LS - 1, t, 0, 0)] = 1.0
-            srcs.append(v)
-    rng = np.random.default_rng(NOISE_SEED + 104729 * rank)
+                v[Ls - 1, t, 0, 0] = 1.0
+            srcs.append(v.ravel())
+    rng = np.random.default_rng(seed)
     phases = np.array([1, 1j, -1, -1j])
     for _ in range(N_NOISE):
-        eta = phases[rng.integers(0, 4, size=(NT, NX, 2))]
-        v = np.zeros((LS, NT, NX, 2), np.complex128)
+        eta = phases[rng.integers(0, 4, size=(Nt, Nx, 2))]
+        v = np.zeros((Ls, Nt, Nx, 2), np.complex128)
         v[0, :, :, 1] = eta[:, :, 1]
-        v[LS - 1, :, :, 0] += eta[:, :, 0]
+        v[Ls - 1, :, :, 0] += eta[:, :, 0]
         srcs.append(v.ravel())
-    for t in WALL_TIMES:
+    for t in (0, Nt // 2):
         for b in (0, 1):
-            v = np.zeros((LS, NT, NX, 2), np.complex128)
+            v = np.zeros((Ls, Nt, Nx, 2), np.complex128)
             if b == 1:
                 v[0, t, :, 1] = 1.0
             else:
-                v[LS - 1, t, :, 0] = 1.0
+                v[Ls - 1, t, :, 0] = 1.0
             srcs.append(v.ravel())
     return np.stack(srcs)
+
+
+def workload_sources(rank):
+    """The workload's 28 boundary sources (boundary_source_set on the bench
+    lattice; the noise seeded per rank)."""
+    return boundary_source_set(NT, NX, LS, NOISE_SEED + 104729 * rank)
 
 
 def sig(x, n=4):
@@ -546,6 +546,103 @@ def analysis_study(nconf=64, therm=10):
 
 # DWF 128x128, Ls = 24, M5 = 1, m_f = 0.02, beta = 4: the larger HMC comparison
 C5_LATTICE, C5_M5, C5_MF, C5_BETA = (128, 128, 24), 1.0, 0.02, 4.0
+
+
+def c5_study(ntraj=200, therm=40, thin=4):
+    """The study's full form at C5 size (DWF 128x128, Ls = 24, M5 = 1,
+    m_f = 0.02, beta = 4): a GPU-HMC chain of ntraj trajectories from a seeded
+    pure-gauge start (the reference generator's loop, epsilon = 0.01, 40
+    leapfrog steps, mixed-CG pseudofermion solves to 1e-10), the configurations
+    from `therm` on, every `thin`-th kept; all their propagators (28 boundary
+    sources per configuration) in one dwf_measure call on the even-odd solver
+    with every contraction and the analyzer's reductions; then the learned
+    preconditioner trained on the first four kept configurations and used on
+    the 28 sources of the fifth, beside the even-odd and plain FP64 solvers on
+    the same sources (all to the FP64 true residual 1e-10). One JSON line."""
+    import torch
+    import three_part_dwf_study_b200 as T
+    from three_part_dwf_study_b200 import analysis
+    from three_part_dwf_study_b200.ensemble import hmc_chain, quenched_theta
+    from three_part_dwf_study_b200.rng import z4_digits
+    Nt, Nx, Ls = C5_LATTICE
+    d = T.DomainWall(Nt, Nx, Ls, C5_M5, C5_MF, C5_BETA)
+    st = torch.cuda.ExternalStream(d.stream_ptr())
+    th0 = quenched_theta(np.random.default_rng(GAUGE_SEED + 5), Nt, Nx, C5_BETA)
+    t0 = time.perf_counter()
+    cfg, hist = hmc_chain(d, th0, ntraj, seed=4321, epsilon=HMC_EPS, steps=HMC_STEPS, rtol=RTOL,
+                          maxiter=50000, solver=T.SOLVER_MIXED, thermalization_cut=therm, thin=thin)
+    hmc_s = time.perf_counter() - t0
+    out = {"lattice": [Nt, Nx, Ls], "M5": C5_M5, "mf": C5_MF, "beta": C5_BETA, "trajectories": ntraj,
+           "epsilon": HMC_EPS, "leapfrog_steps": HMC_STEPS, "rtol": RTOL,
+           "hmc_seconds_per_trajectory": sig(hmc_s / ntraj),
+           "acceptance": sig(float(hist["accepted"].mean())),
+           "plaquette_mean_after_thermalisation": sig(float(hist["plaquette"][therm:].mean())),
+           "plaquette_std_after_thermalisation": sig(float(hist["plaquette"][therm:].std())),
+           "max_abs_dH": sig(float(np.abs(hist["dH"]).max())), "configurations_kept": len(cfg)}
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        r = fn()
+        e1.record(st)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1) * 1e-3
+
+    # the kept configurations in calls of 8 (224 right-hand sides per call: the
+    # solver's workspace for all of them at once would not fit the device)
+    nconf = len(cfg)
+    parts, sec = [], 0.0
+    for c0 in range(0, nconf, 8):
+        blk = cfg[c0:c0 + 8]
+        z4 = np.concatenate([z4_digits(NOISE_SEED + 104729 * k, N_NOISE * Nt * Nx * 2)
+                             for k in range(c0, c0 + len(blk))])
+        kw = dict(z4=z4, n_point_times=4, n_wall_times=2, n_noise=N_NOISE, max_momentum=5, rtol=RTOL,
+                  maxiter=50000, solver=T.SOLVER_EO_MIXED)
+        mb, sb = timed(lambda: d.measure(blk, **kw))
+        parts.append(mb)
+        sec += sb
+    m = {k: np.concatenate([p[k] for p in parts]) for k in ("cpp", "cj5", "loop", "mom_cpp")}
+    m["info"] = [i for p in parts for i in p["info"]]
+    if not all(i["converged"] for i in m["info"]):
+        raise SystemExit("C5 study: a measurement solve did not converge")
+    red = analysis.reduce_ensemble(m, Nt, Nx, 2)
+    nr = len(m["info"])
+    out["measurement"] = {"rhs": nr, "configurations_per_call": 8, "seconds": sig(sec),
+                          "solves_per_s": sig(nr / sec),
+                          "ms_per_configuration": sig(1e3 * sec / nconf),
+                          "schur_iterations_mean": sig(statistics.mean(i["schur_iterations"] for i in m["info"])),
+                          "m_res": sig(red["m_res_average"])}
+    # learned preconditioner on the chain's own configurations
+    d.set_gauge(np.stack(cfg[:4]))
+    d.lp_init(hidden=LP_HIDDEN, seed=5)
+    t0 = time.perf_counter()
+    d.lp_train(**LP_TRAIN)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    d.set_gauge(cfg[4])
+    src = torch.from_numpy(boundary_source_set(Nt, Nx, Ls, NOISE_SEED).view(np.float64).copy()).cuda()
+    x = torch.zeros_like(src)
+    res = {}
+    for name, sv in (("learned", T.SOLVER_LEARNED), ("even_odd_mixed", T.SOLVER_EO_MIXED),
+                     ("plain_fp64_cg", T.SOLVER_CG64)):
+        d.propagators_dev(src, x, rtol=RTOL, maxiter=50000, solver=sv)  # warm-up (tuning)
+        infos, sec = timed(lambda: d.propagators_dev(src, x, rtol=RTOL, maxiter=50000, solver=sv))
+        if not all(i["converged"] and i["true_relres"] <= RTOL * 1.0001 for i in infos):
+            raise SystemExit(f"C5 study: {name} solve did not reach the FP64 true residual")
+        res[name] = {"solves_per_s": sig(src.shape[0] / sec),
+                     "iterations_mean": sig(statistics.mean(
+                         (i["schur_iterations"] if sv != T.SOLVER_CG64 else i["iterations"]) for i in infos)),
+                     "fallbacks": sum(i["fallback"] for i in infos)}
+    res["learned_training_s"] = sig(train_s)
+    res["learned_speedup_vs_plain_fp64"] = sig(res["learned"]["solves_per_s"] / res["plain_fp64_cg"]["solves_per_s"])
+    res["even_odd_speedup_vs_plain_fp64"] = sig(res["even_odd_mixed"]["solves_per_s"]
+                                                / res["plain_fp64_cg"]["solves_per_s"])
+    out["propagators_28_sources"] = res
+    d.close()
+    print(json.dumps({"c5_study": out}))
+    return 0
 
 
 def hmc_compare_large(T, local, ntraj):
@@ -1264,11 +1361,15 @@ def main():
     ap.add_argument("--eo-phases", action="store_true")
     ap.add_argument("--analysis-study", action="store_true",
                     help="64 GPU-HMC configurations per Nx in {32,56,80,96}, all propagators in one call")
+    ap.add_argument("--c5-study", action="store_true",
+                    help="200 GPU-HMC trajectories at 128x128x24, their analysis and the learned solver there")
     ap.add_argument("--cpu-reference-extras", action="store_true",
                     help="time the reference's own HMC trajectory (B4) and analyzer (B6) on the host cores")
     args = ap.parse_args()
     if args.cpu_reference_extras:
         return cpu_reference_extras()
+    if args.c5_study:
+        return c5_study()
     if args.profile_case:
         return profile_case()
     if args.profile_dslash:

@@ -427,7 +427,7 @@ uint64_t dwf_graph_replays(const dwf_ctx* ctx, int* cached);
  * values and the weights are rounded to BF16, the products accumulated in FP32
  * on the tensor cores. Weights: 2 * dwf_lp_weights_size floats (re, im), layer
  * by layer, each [9][cout][cin]. */
-int dwf_lp_init(dwf_ctx* ctx, int hidden, uint64_t seed);   /* hidden: 8, 16, 24 or 32 */
+int dwf_lp_init(dwf_ctx* ctx, int hidden, uint64_t seed);   /* hidden: 8, 16, 24 or 32; 2 Ls hidden <= 1536, Ls <= 24 */
 int dwf_lp_weights_size(const dwf_ctx* ctx, long* n_complex);
 int dwf_lp_get_weights(dwf_ctx* ctx, float* w);
 int dwf_lp_set_weights(dwf_ctx* ctx, const float* w);

@@ -129,6 +129,34 @@ def test_loss_and_gradient_match_oracle(T, torch, variant):
     d.close()
 
 
+def test_gradient_matches_oracle_at_the_widest_layers(T, torch):
+    """Ls = 24 with 32 hidden channels (48 x 32 complex weights per offset,
+    the weight-gradient kernel's wider per-thread tiling): loss and gradient
+    against the oracle's rounded network."""
+    d, th, ws = setup_dwf(T, Nt=8, Nx=12, Ls=24, hidden=32)
+    rng = np.random.default_rng(31)
+    V, C0 = d.Nt * d.Nx, 2 * d.Ls
+    nb = LN.neighbours(d.Nt, d.Nx)
+    rho = crand(rng, 2, d.Ndof)
+    e = crand(rng, 2, d.Ndof)
+    conf = np.array([0, 1], np.int32)
+    loss, grads = d.lp_loss_grad_dev(torch.from_numpy(rho).cuda(), torch.from_numpy(e).cuda(),
+                                     pair_conf=conf)
+    lo = 0.0
+    go = [np.zeros_like(w, dtype=np.complex128) for w in ws]
+    for b in range(2):
+        Tg = d.lp_transports(int(conf[b])).astype(np.complex128)
+        lb, gb = LN.loss_grad(Tg, nb, ws, LN.to_net(rho[b:b + 1], V, C0), LN.to_net(e[b:b + 1], V, C0),
+                              rounded=True)
+        lo += lb / 2
+        for l in range(4):
+            go[l] += gb[l] / 2
+    assert abs(loss - lo) < 1e-5 * abs(lo)
+    for l in range(4):
+        assert rel(grads[l], go[l]) < 2e-3, l
+    d.close()
+
+
 @pytest.mark.parametrize("Ls,hidden,Nt,Nx", [(16, 32, 16, 64), (12, 24, 16, 64), (24, 16, 16, 64),
                                           (20, 24, 16, 64), (16, 32, 4, 256)])
 def test_layer_variants_agree_at_wide_layers(T, torch, Ls, hidden, Nt, Nx):

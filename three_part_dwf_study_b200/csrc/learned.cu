@@ -960,10 +960,14 @@ struct GradArgs
 
 constexpr int kGradSites = 32;
 constexpr int kGradThreads = 256;
-constexpr int kGradMaxPer = 4;  // cout * cin <= kGradThreads * kGradMaxPer
+// weights per thread: cout * cin <= kGradThreads * PER; 4 for layers up to
+// 1024 complex weights per offset, 6 up to 1536 (48 x 32: Ls = 24, 32 hidden)
+constexpr int kGradMaxPer = 6;
 
+template <int PER>
 __global__ void __launch_bounds__(kGradThreads) lp_wgrad_kernel(GradArgs a)
 {
+    constexpr int kGradMaxPer = PER;
     extern __shared__ __align__(16) unsigned char smem[];
     float2* gs = reinterpret_cast<float2*>(smem);      // [32][cout]
     float2* as = gs + kGradSites * a.cout;             // [32][cin]
@@ -2367,7 +2371,10 @@ int lp_loss_grad(dwf_ctx* c, int nrhs, const int* conf_d, const float2* rho, con
         a.nrhs = nrhs;
         a.part = n->gpart;
         const size_t smem = size_t(kGradSites) * (a.cin + a.cout) * sizeof(float2);
-        lp_wgrad_kernel<<<nblk_g, kGradThreads, smem, c->stream>>>(a);
+        if (a.cin * a.cout <= kGradThreads * 4)
+            lp_wgrad_kernel<4><<<nblk_g, kGradThreads, smem, c->stream>>>(a);
+        else
+            lp_wgrad_kernel<kGradMaxPer><<<nblk_g, kGradThreads, smem, c->stream>>>(a);
         const int E = 9 * a.cin * a.cout;
         lp_grad_reduce_kernel<<<(E + 255) / 256, 256, 0, c->stream>>>(n->gpart, nblk_g, E, n->G + n->woff[l]);
         c->launches += 2;
@@ -3006,7 +3013,7 @@ int dwf_lp_init(dwf_ctx* c, int hidden, uint64_t seed)
         return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: hidden must be 8, 16, 24 or 32");
     const int C0 = 2 * c->L.Ls;
     if (C0 > 48 || C0 * hidden > kGradThreads * kGradMaxPer)
-        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: 2*Ls*hidden must be <= 1024 and Ls <= 24");
+        return ctx_fail(c, DWF_BAD_ARG, "dwf_lp_init: 2*Ls*hidden must be <= 1536 and Ls <= 24");
     CK(cudaSetDevice(c->device));
     lp_destroy(c);
     LpNet* n = new LpNet();

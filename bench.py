@@ -557,8 +557,9 @@ def c5_study(ntraj=200, therm=40, thin=4):
     sources per configuration) in one dwf_measure call on the even-odd solver
     with every contraction and the analyzer's reductions; then the learned
     preconditioner trained on the first four kept configurations and used on
-    the 28 sources of the fifth, beside the even-odd and plain FP64 solvers on
-    the same sources (all to the FP64 true residual 1e-10). One JSON line."""
+    the 28 sources of the fifth (flexible GCR restarted every 4 and every 16
+    iterations), beside the even-odd and plain FP64 solvers on the same
+    sources (all to the FP64 true residual 1e-10). One JSON line."""
     import torch
     import three_part_dwf_study_b200 as T
     from three_part_dwf_study_b200 import analysis
@@ -625,8 +626,10 @@ def c5_study(ntraj=200, therm=40, thin=4):
     src = torch.from_numpy(boundary_source_set(Nt, Nx, Ls, NOISE_SEED).view(np.float64).copy()).cuda()
     x = torch.zeros_like(src)
     res = {}
-    for name, sv in (("learned", T.SOLVER_LEARNED), ("even_odd_mixed", T.SOLVER_EO_MIXED),
-                     ("plain_fp64_cg", T.SOLVER_CG64)):
+    for name, sv, restart in (("learned", T.SOLVER_LEARNED, 4), ("learned_gcr16", T.SOLVER_LEARNED, 16),
+                              ("even_odd_mixed", T.SOLVER_EO_MIXED, 4),
+                              ("plain_fp64_cg", T.SOLVER_CG64, 4)):
+        d.lp_set_krylov(T.LP_GCR, restart)
         d.propagators_dev(src, x, rtol=RTOL, maxiter=50000, solver=sv)  # warm-up (tuning)
         infos, sec = timed(lambda: d.propagators_dev(src, x, rtol=RTOL, maxiter=50000, solver=sv))
         if not all(i["converged"] and i["true_relres"] <= RTOL * 1.0001 for i in infos):

@@ -607,7 +607,7 @@ constexpr int kProdWarps = 3;
 template <int NCOL>
 __global__ void __launch_bounds__(kTcThreads, 2) lp_tc_kernel(TcArgs a)
 {
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char tc_smem[];
     constexpr int kSlots = 4;
     __shared__ __align__(8) uint64_t mbar[2 * kSlots + 6];
     __shared__ uint32_t tmem_holder;
@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) lp_tc_kernel(TcArgs a)
     const int P = a.Nx + 2;                 // padded rows per lattice row
     const int J = tc_window_rows(a.Nx);     // staged rows per tile
     const long NP = long(a.Nt) * P;         // padded rows per right-hand side
-    uint4* Bs = reinterpret_cast<uint4*>(smem);
+    uint4* Bs = reinterpret_cast<uint4*>(tc_smem);
     uint4* As = Bs + nks * 2 * NCOL;        // [buffer][plane][row]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t mb = smem_u32(&mbar[0]);
@@ -1653,9 +1653,9 @@ __global__ void __launch_bounds__(256) lp_gcr_update_kernel(GcrArgs g)
     __shared__ bool last;
     const int rhs = blockIdx.y, nrhs = gridDim.y;
     GcrState* st = g.S + rhs;
-    if (threadIdx.x <= NV)
+    if (int(threadIdx.x) <= NV)
     {
-        const double2 c = threadIdx.x < NV ? st->beta[NV][threadIdx.x] : st->alpha[NV];
+        const double2 c = int(threadIdx.x) < NV ? st->beta[NV][threadIdx.x] : st->alpha[NV];
         cb[threadIdx.x] = make_float2(float(c.x), float(c.y));
     }
     __syncthreads();

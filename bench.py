@@ -669,29 +669,36 @@ def hmc_compare_large(T, local, ntraj):
 
 def wilson_learned_grid(T, ntrain=8):
     """Wilson 64x64 near the critical mass: the learned preconditioner (4
-    layers, 8 hidden complex channels) trained on ntrain seeded configurations
-    per (beta, m0), then 16 point-source propagator solves to 1e-10 on a
-    held-out configuration, against the plain FP64 CG (CGNR) and the mixed CG
+    layers, 8 hidden complex channels) trained on ntrain configurations of a
+    GPU Wilson-HMC chain per (beta, m0), then 16 point-source propagator solves
+    to 1e-10 on the chain's next configuration, against the plain FP64 CG (CGNR) and the mixed CG
     on the same GPU. Device time per batch (CUDA events on the library
     stream, host copies of sources and solutions included), iterations and
     operator applications."""
     import torch
-    from three_part_dwf_study_b200.ensemble import quenched_ensemble
+    from three_part_dwf_study_b200.ensemble import quenched_theta, wilson_hmc_chain
     L = 64
-    out = {"lattice": [L, L], "hidden": 8, "sources": 16, "rtol": RTOL, "settings": {}}
+    out = {"lattice": [L, L], "hidden": 8, "sources": 16, "rtol": RTOL,
+           "configurations": "Wilson HMC chain per setting (trajectory length 0.1 in 20 steps, CG to "
+                             "1e-10) from a pure-gauge start: 10 thermalisation trajectories, then "
+                             f"{ntrain} training configurations and one held out", "settings": {}}
     for beta in (2.0, 3.0, 4.0, 6.0):
         for m0 in (-0.05, 0.05):
             w = T.Wilson(L, L, m0, beta)
             st = torch.cuda.ExternalStream(w.stream_ptr())
-            w.set_gauge(quenched_ensemble(GAUGE_SEED + int(10 * beta), ntrain, L, L, beta))
+            th0 = quenched_theta(np.random.default_rng(GAUGE_SEED + int(10 * beta)), L, L, beta)
+            cfg, hist = wilson_hmc_chain(w, th0, 10 + ntrain + 1, seed=GAUGE_SEED + int(100 * (beta + m0)),
+                                         epsilon=0.1 / 20, steps=20, tolerance=RTOL, max_iterations=50000,
+                                         solver=T.SOLVER_MIXED, thermalization_cut=10)
+            w.set_gauge(cfg[:ntrain])
             w.lp_init(hidden=8, seed=1)
             tinfo = w.lp_train(steps=3000, batch=8, lr=3e-3, lr_decay_steps=1000, pairs_per_conf=32,
                                solver_iters=50, solver_every=2, seed=3)
-            w.set_gauge(quenched_ensemble(GAUGE_SEED + 7 + int(10 * beta), 1, L, L, beta))
+            w.set_gauge(cfg[ntrain])
             src = np.zeros((16, w.Ndof), np.complex128)
             for k in range(16):
                 src[k, ((4 * k) * L) * 2 + (k % 2)] = 1.0
-            row = {"training_loss": tinfo["loss_last"]}
+            row = {"training_loss": tinfo["loss_last"], "hmc_acceptance": float(hist["accepted"].mean())}
             for name, sv in (("learned", T.SOLVER_LEARNED), ("plain_fp64_cg", T.SOLVER_CG64),
                              ("mixed_cg", T.SOLVER_MIXED)):
                 w.propagators(src, rtol=RTOL, maxiter=50000, solver=sv)

@@ -70,6 +70,39 @@ def test_wilson_32x32_chain_matches_oracle(T, wilson_oracle_chain, solver):
     w.close()
 
 
+def test_wilson_hmc_chain_helper_matches_oracle(T):
+    """ensemble.wilson_hmc_chain (the chain that generates the Wilson
+    learned-preconditioner grid's configurations): its draws replayed through
+    the oracle's hmc_step give the same decisions, dH and configurations, and
+    the thermalisation cut and thinning keep the right trajectories."""
+    from three_part_dwf_study_b200.ensemble import wilson_hmc_chain
+    Nt = Nx = 16
+    beta, m0, eps, steps, ntraj = 2.0, 0.1, 0.05, 20, 6
+    w = T.Wilson(Nt, Nx, m0, beta)
+    th0 = np.random.default_rng(7).uniform(-np.pi, np.pi, w.Ngauge)
+    cfg, hist = wilson_hmc_chain(w, th0, ntraj, seed=99, epsilon=eps, steps=steps, tolerance=1e-10,
+                                 max_iterations=4000, thermalization_cut=2, thin=2)
+    assert cfg.shape == (2, w.Ngauge)
+    o = O.Wilson(Nt, Nx, m0)
+    rng = np.random.default_rng(99)
+    cur = th0.copy()
+    kept = []
+    for k in range(ntraj):
+        mom = rng.normal(size=w.Ngauge)
+        chi = (rng.normal(size=w.Ndof) + 1j * rng.normal(size=w.Ndof)) / np.sqrt(2.0)
+        u = rng.uniform()
+        st, cur, inf = o.hmc_step(beta, eps, steps, 1e-10, 4000, cur, mom, chi, u)
+        assert st == 0
+        assert bool(inf["accepted"]) == bool(hist["accepted"][k]), k
+        assert abs(inf["dH"] - hist["dH"][k]) < 1e-6, k
+        if k >= 2 and (k - 2) % 2 == 0:
+            kept.append(cur.copy())
+    for a, b in zip(cfg, kept):
+        assert rel(a, b) < 1e-7
+    assert np.all(np.isfinite(hist["plaquette"]))
+    w.close()
+
+
 # ---------------------------------------------------------------------------
 # Domain wall: GPU-HMC configurations measured on both sides
 # ---------------------------------------------------------------------------

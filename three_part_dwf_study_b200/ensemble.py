@@ -75,3 +75,36 @@ def hmc_chain(d, theta0, trajectories, seed, epsilon, steps, rtol=1e-10, maxiter
             kept.append(th.copy())
     configs = np.stack(kept) if kept else np.zeros((0, d.Ngauge))
     return configs, hist
+
+
+def wilson_hmc_chain(w, theta0, trajectories, seed, epsilon, steps, tolerance=1e-10,
+                     max_iterations=5000, solver=None, thermalization_cut=0, thin=1):
+    """A Wilson pseudofermion HMC Markov chain on the GPU: per trajectory,
+    from one numpy generator seeded with `seed`, the momenta (2 Nt Nx normals),
+    the pseudofermion chi (Ndof complex normals, variance 1/2 per part) and the
+    Metropolis uniform, then Wilson.hmc_step (leapfrog and accept/reject,
+    wilson/include/gauge.hpp:132-180). Configurations from trajectory
+    `thermalization_cut` on, every `thin`-th, are kept.
+
+    w: Wilson context. Returns (configs [n][2 Nt Nx], history) with history a
+    dict of per-trajectory arrays accepted, dH, plaquette."""
+    from . import _capi as A
+
+    solver = A.SOLVER_CG64 if solver is None else solver
+    rng = np.random.default_rng(seed)
+    th = np.ascontiguousarray(theta0, dtype=np.float64).reshape(-1).copy()
+    kept = []
+    hist = {k: np.zeros(trajectories) for k in ("accepted", "dH", "plaquette")}
+    for k in range(trajectories):
+        mom = rng.normal(size=w.Ngauge)
+        chi = (rng.normal(size=w.Ndof) + 1j * rng.normal(size=w.Ndof)) / np.sqrt(2.0)
+        u = rng.uniform()
+        th, info = w.hmc_step(th, mom, chi, u, epsilon, steps, tolerance, max_iterations,
+                              solver=solver)
+        hist["accepted"][k] = info["accepted"]
+        hist["dH"][k] = info["dH"]
+        hist["plaquette"][k] = w.average_plaquette(th)
+        if k >= thermalization_cut and (k - thermalization_cut) % thin == 0:
+            kept.append(th.copy())
+    configs = np.stack(kept) if kept else np.zeros((0, w.Ngauge))
+    return configs, hist

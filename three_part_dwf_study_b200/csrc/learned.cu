@@ -413,6 +413,10 @@ struct TcArgs
 
 constexpr int kTcM = 128;
 
+#ifndef DWFB_TC_PDL
+#define DWFB_TC_PDL 1  // layer kernels launched as programmatic dependents of their predecessor
+#endif
+
 // Staged window of one tile in padded rows: lattice rows stored with one
 // halo site on each side (P = Nx + 2 rows per lattice row), the tile's 128
 // rows plus one padded lattice row and one site on each side.
@@ -657,6 +661,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) lp_tc_kernel(TcArgs a)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_holder;
+    // Launched as a programmatic dependent of the previous kernel on the
+    // stream, the prologue above (weights, barriers, TMEM) may run while that
+    // kernel finishes; every thread waits here for its completion before any
+    // field is read or written, then lets the next layer's CTAs start their own
+    // prologue (they take an SM only as this grid's CTAs leave it).
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const long tiles_per_rhs = tc_tiles_per_rhs(a.Nt, a.Nx);
     const long ntiles = tiles_per_rhs * a.nrhs;
     bool ok = true;
@@ -2163,13 +2174,25 @@ int lp_layer(dwf_ctx* c, int l, bool adjoint, int nrhs, const int* conf_d, const
         const long ntiles = tc_tiles_per_rhs(c->L.Nt, c->L.Nx) * nrhs;
         const int grid = int(std::max<long>(1, std::min<long>(ntiles, long(two ? 2 : 1) * c->nsm)));
         ST(set_conv_smem(c));
+        // programmatic dependent launch (the kernel waits for its predecessor
+        // before touching any field; see lp_tc_kernel)
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = DWFB_TC_PDL;
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(kTcThreads);
+        cfg.dynamicSmemBytes = tsm;
+        cfg.stream = c->stream;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
         switch (ncol)
         {
-        case 16: lp_tc_kernel<16><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
-        case 32: lp_tc_kernel<32><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
-        case 48: lp_tc_kernel<48><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
-        case 64: lp_tc_kernel<64><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
-        case 96: lp_tc_kernel<96><<<grid, kTcThreads, tsm, c->stream>>>(t); break;
+        case 16: CK(cudaLaunchKernelEx(&cfg, lp_tc_kernel<16>, t)); break;
+        case 32: CK(cudaLaunchKernelEx(&cfg, lp_tc_kernel<32>, t)); break;
+        case 48: CK(cudaLaunchKernelEx(&cfg, lp_tc_kernel<48>, t)); break;
+        case 64: CK(cudaLaunchKernelEx(&cfg, lp_tc_kernel<64>, t)); break;
+        case 96: CK(cudaLaunchKernelEx(&cfg, lp_tc_kernel<96>, t)); break;
         default: return ctx_fail(c, DWF_BAD_ARG, "learned: unsupported channel count");
         }
         c->launches += 1;

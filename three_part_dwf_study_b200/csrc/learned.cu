@@ -1564,6 +1564,8 @@ __global__ void __launch_bounds__(256) lp_gcr_dots_kernel(GcrArgs g)
     constexpr int NVAL = 3 + 4 * NV;
     __shared__ double sred[8][NVAL];
     __shared__ double tot[NVAL];
+    // launched as a programmatic dependent: the previous kernel's results first
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     __shared__ bool last;
     const int rhs = blockIdx.y;
     const long ch = (g.f4 + g.nblk - 1) / g.nblk;
@@ -1662,6 +1664,7 @@ __global__ void __launch_bounds__(256) lp_gcr_update_kernel(GcrArgs g)
     __shared__ float2 cb[NV + 1];  // beta_k0 .. beta_k(k-1), alpha_k
     __shared__ double red[32];
     __shared__ bool last;
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // as lp_gcr_dots_kernel
     const int rhs = blockIdx.y, nrhs = gridDim.y;
     GcrState* st = g.S + rhs;
     if (int(threadIdx.x) <= NV)
@@ -1743,6 +1746,7 @@ __global__ void __launch_bounds__(256) lp_gcr_update_kernel(GcrArgs g)
 __global__ void __launch_bounds__(256) lp_gcr_x_kernel(GcrArgs g, int m)
 {
     __shared__ float2 gam[kGcrMax];
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // as lp_gcr_dots_kernel
     const int rhs = blockIdx.y;
     const GcrState* st = g.S + rhs;
     if (threadIdx.x == 0)
@@ -2475,11 +2479,29 @@ int lp_ensure_gcr(dwf_ctx* c, int nrhs, int m)
     return DWF_OK;
 }
 
+// 256-thread launch as a programmatic dependent of the previous kernel on the
+// stream (the kernel waits for it with griddepcontrol.wait before its first
+// access); launch errors surface at the caller's cudaGetLastError.
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), dim3 grid, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <int K>
 void gcr_passes(const GcrArgs& g, dim3 grid, cudaStream_t s)
 {
-    lp_gcr_dots_kernel<K><<<grid, 256, 0, s>>>(g);
-    lp_gcr_update_kernel<K><<<grid, 256, 0, s>>>(g);
+    launch_pdl(lp_gcr_dots_kernel<K>, grid, s, g);
+    launch_pdl(lp_gcr_update_kernel<K>, grid, s, g);
 }
 
 void gcr_passes_k(int k, const GcrArgs& g, dim3 grid, cudaStream_t s)
@@ -2572,7 +2594,7 @@ int lp_gcr_inner(dwf_ctx* c, int nrhs, const int* conf_d, const std::vector<int>
             ST(iter(k));
         if (k0 + 4 == m)
         {
-            lp_gcr_x_kernel<<<grid, 256, 0, c->stream>>>(g, m);
+            launch_pdl(lp_gcr_x_kernel, grid, c->stream, g, m);
             c->launches += 1;
         }
         CK(cudaGetLastError());
@@ -2638,7 +2660,7 @@ int lp_gcr_inner(dwf_ctx* c, int nrhs, const int* conf_d, const std::vector<int>
     if (kc != 0)
     {
         // a cycle cut short: its correction from the iterations launched
-        lp_gcr_x_kernel<<<grid, 256, 0, c->stream>>>(g, kc);
+        launch_pdl(lp_gcr_x_kernel, grid, c->stream, g, kc);
         c->launches += 1;
         CK(cudaMemcpyAsync(fl.data(), n->g_flags, 2 * nrhs * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));

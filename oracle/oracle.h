@@ -3,8 +3,8 @@
  * A plain C++ restatement of the reference's arithmetic with every lattice
  * parameter passed explicitly (the reference reads them from ./parameters.txt
  * at static-initialisation time). Only tests/, __graft_entry__.smoke() and
- * bench.py's CPU-baseline leg load this library, and only as a checker or as
- * the timed CPU baseline; the product never calls it.
+ * bench.py's CPU-baseline leg load this library, and only to check GPU results
+ * or as the timed CPU baseline; the product never calls it.
  *
  * Conventions (identical to the reference):
  *   gauge theta   : double[2*Nt*Nx], index (mu*Nt + t)*Nx + x        (domain_wall/include/indexing.hpp:10-13)

@@ -1,8 +1,8 @@
 """ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
 Loads oracle/liboracle.so (built by ``make -C oracle oracle``). Only tests/,
-__graft_entry__.smoke() and bench.py's CPU-baseline leg import this module, as
-the checker or the timed CPU baseline; the product never does.
+__graft_entry__.smoke() and bench.py's CPU-baseline leg import this module, to
+check GPU results or as the timed CPU baseline; the product never does.
 
 Complex arrays are numpy complex128 in the reference layouts:
 DWF fields  : flat [Ls*Nt*Nx*2], index ((s*Nt+t)*Nx+x)*2+spin

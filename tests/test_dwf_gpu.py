@@ -3,7 +3,7 @@ CPU oracle and the reference's golden vectors.
 
 Tolerances: FP64 operator outputs within 1e-13 relative (different
 summation order and FMA contraction only); FP64 CG solutions within 1e-12
-relative when both solve to rtol 1e-13; the mixed path is judged by its FP64
+relative when both solve to rtol 1e-13; the mixed path is checked by its FP64
 true residual."""
 import numpy as np
 import pytest

@@ -1136,7 +1136,8 @@ def profile_learned():
 def profile_dslash():
     """One application of D at the Dslash bench lattice for each kernel
     variant (site, column, site with shuffled x neighbours, t sweep, column
-    with shuffled x neighbours) in FP64, then in FP32 (for ncu)."""
+    with shuffled x neighbours, slice ring fed by bulk copies) in FP64, then in
+    FP32 (for ncu)."""
     import torch
     import three_part_dwf_study_b200 as T
     from three_part_dwf_study_b200 import _capi as A
@@ -1146,7 +1147,7 @@ def profile_dslash():
     for dt in (torch.float64, torch.float32):
         a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
         b = torch.empty_like(a)
-        for v in (0, 1, 2, 3, 5):
+        for v in (0, 1, 2, 3, 5, 6):
             A.check(A.lib().dwf_set_dslash_variant(d.handle, v), d.handle)
             d.apply_dev(0, a, b)
     d.sync()
@@ -1318,6 +1319,7 @@ def dslash_variants():
             a = torch.randn(d.Ndof * 2, dtype=dt, device="cuda")
             b = torch.empty_like(a)
             kinds = [(0, 0, "site"), (1, 0, "column"), (2, 0, "site_shuffle"), (5, 0, "column_shuffle"),
+                     (6, 0, "slice_ring"),
                      (3, 0, "t_sweep_auto"), (3, 8, "t_sweep_8"), (3, 16, "t_sweep_16"),
                      (3, 32, "t_sweep_32"), (3, 64, "t_sweep_64")]
             if Dl == 1:

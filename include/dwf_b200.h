@@ -356,8 +356,14 @@ int dwf_barrier_selftest(dwf_ctx* ctx, int missing_blocks, uint64_t limit_ns);
  * consecutive rows of one column, all loads up front into registers (Nx a
  * multiple of 32 and Nt of 4; else as 0), 5 = as 1 with the x neighbours
  * exchanged by warp shuffles and the next slice's loads issued ahead (Nx a
- * multiple of 32; else as 1), -1 = autotune (default): the first
- * application per (precision, batch-size bucket) times the variants with
+ * multiple of 32; else as 1), 6 = as 1 with each block's slices (its 32 x 8
+ * sites and their halo) brought into a shared-memory ring by 1-D bulk copies
+ * completing on mbarriers, every neighbour read from shared memory (Nx a
+ * multiple of 32 and Nt of 8; else as 0; chosen only by this call: slower
+ * than 5 at the sizes measured; a copy wait that runs past the context's
+ * timeout leaves the output incomplete and DWF_TIMEOUT in the device error
+ * word that the next solve reports), -1 = autotune (default): the first
+ * application per (precision, batch-size bucket) times variants 0-5 with
  * CUDA events and keeps the fastest, variant 3 at its automatic shape and at
  * chunks of 16, 32, 64 and 128 rows with the widest, a half- and a
  * quarter-width block (unless dwf_set_dslash_chunk fixes the chunk). dwf_dslash_variant reports the choice in force for a

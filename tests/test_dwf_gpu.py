@@ -199,9 +199,10 @@ def test_bounded_barrier_times_out_and_context_survives(tdwf):
     assert r.converged and r.info["true_relres"] < 1e-9
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("shape", [(8, 8, 4), (13, 37, 3), (64, 64, 16), (5, 3, 1), (16, 40, 24),
-                                   (6, 32, 2), (3, 96, 5), (9, 128, 4), (20, 64, 1)])
+                                   (6, 32, 2), (3, 96, 5), (9, 128, 4), (20, 64, 1), (8, 32, 3),
+                                   (16, 96, 1), (24, 64, 5)])
 def test_dslash_variants_match_oracle(tdwf, variant, shape):
     """The Dslash kernels (one thread per 5-D site; one thread per 4-D site
     sweeping the fifth dimension; one thread per 5-D site with warp-shuffled x
@@ -209,8 +210,10 @@ def test_dslash_variants_match_oracle(tdwf, variant, shape):
     thread per (s, x) sweeping a chunk of rows in t, which takes Nx % 32 == 0
     and Ls <= 16 and otherwise runs as the first; the Wilson-only row kernel,
     which runs as the first on domain wall; the column kernel with shuffled x
-    neighbours, which takes Nx % 32 == 0 and otherwise runs as the second) in
-    FP64 and FP32, ragged
+    neighbours, which takes Nx % 32 == 0 and otherwise runs as the second; the
+    slice-ring kernel fed by bulk copies, which takes Nx % 32 == 0 and
+    Nt % 8 == 0 and otherwise runs as the first: 8x32x3 is one block whose
+    halo rows and columns all wrap) in FP64 and FP32, ragged
     tile edges, row/warp boundaries, several x tiles per block (9x128x4,
     20x64x1) and ragged t chunks included."""
     torch = pytest.importorskip("torch")
@@ -257,7 +260,7 @@ def test_dslash_sweep_chunks(tdwf, chunk, shape):
     assert A.lib().dwf_set_dslash_chunk(d.handle, -1) != 0
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("shape", [(16, 256), (7, 96), (12, 64), (4, 32), (8, 32), (36, 160)])
 def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
     """The Wilson operator (no fifth dimension, antiperiodic in both
@@ -284,7 +287,7 @@ def test_wilson_dslash_variants_match_oracle(tdwf, variant, shape):
         assert rel(y32.cpu().numpy(), ref) < 2e-6, name
     assert w.dslash_variant(32, 2) == variant
     with pytest.raises(A.DwfError):
-        w.set_dslash_variant(6)
+        w.set_dslash_variant(7)
 
 
 def test_wilson_dslash_autotuned_matches_oracle(tdwf):
@@ -313,14 +316,14 @@ def test_wilson_dslash_autotuned_matches_oracle(tdwf):
             assert A.lib().dwf_dslash_variant(w.handle, prec, nf) in (0, 1, 2, 3, 4, 5)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 def test_dslash_unaligned_fields(tdwf, variant):
     """FP64 fields that start 16 bytes past a 32-byte boundary (a view one
     complex number into a buffer) take the kernels' 16-byte access path; the
     results equal those of aligned fields."""
     torch = pytest.importorskip("torch")
     from three_part_dwf_study_b200 import _capi as A
-    Nt, Nx, Ls = 12, 64, 4
+    Nt, Nx, Ls = (16 if variant == 6 else 12), 64, 4  # the slice ring takes Nt % 8 == 0
     rng = np.random.default_rng(77 + variant)
     d = tdwf.DomainWall(Nt, Nx, Ls, 1.3, 0.02)
     o = O.Dwf(Nt, Nx, Ls, 1.3, 0.02)

@@ -142,6 +142,7 @@ namespace {
 // One application of D (dag = false) or D^dag with the chosen kernel variant.
 // The t-sweeping kernel needs whole 32-lane rows and a block of all Ls slices.
 bool sweep_ok(const Lat& L) { return L.Nx % 32 == 0 && 32 * L.Ls <= 512; }
+bool tile_ok(const Lat& L) { return L.Nx % 32 == 0 && L.Nt % kRingT == 0; }
 bool wilson_rows_ok(const Lat& L)
 {
     return L.Ls == 1 && !L.fifth && L.Nx % 32 == 0 && L.Nt % kWilsonRows == 0;
@@ -268,6 +269,27 @@ void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* co
         prefer_l1(c, 0 + (dag ? 1 : 0) + (sizeof(R) == 8 ? 2 : 0), kern);
         kern<<<grid, 256, 0, c->stream>>>(c->L, in, out, fs, U, c->usz(), conf_d, conf0);
     }
+    else if (variant == 6 && tile_ok(c->L) && c->dslash_err)
+    {
+        const dim3 grid(c->L.Nx / 32, c->L.Nt / kRingT, nrhs);
+        auto kern = dag ? dirac_tile_kernel<true, R> : dirac_tile_kernel<false, R>;
+        const int bit = 8 + (dag ? 1 : 0) + (sizeof(R) == 8 ? 2 : 0);
+        if (!(c->sweep_smem_set & (1 << bit)))
+        {
+            // several blocks' rings per SM need the largest shared-memory split;
+            // a refusal only leaves fewer blocks resident
+            const bool clean = cudaPeekAtLastError() == cudaSuccess;
+            if ((cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      int(cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
+                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(tile_smem_bytes(2 * sizeof(cplx<R>)))) != cudaSuccess) &&
+                clean)
+                cudaGetLastError();
+            c->sweep_smem_set |= 1 << bit;
+        }
+        kern<<<grid, 256, tile_smem_bytes(2 * sizeof(cplx<R>)), c->stream>>>(
+            c->L, in, out, fs, U, c->usz(), conf_d, conf0, c->dslash_err, c->timeout_ns);
+    }
     else if (variant == 1 || variant == 5)
     {
         const dim3 grid((c->L.Nx + 31) / 32, (c->L.Nt + 7) / 8, nrhs);
@@ -305,7 +327,8 @@ void launch_dirac(dwf_ctx* c, DslashChoice ch, bool dag, int nrhs, const int* co
 // site with warp-shuffled x neighbours (Nx a multiple of 32), 3 one thread per
 // (s, x) sweeping a chunk of rows in t (Nx a multiple of 32, Ls <= 16), 4 (Wilson
 // only) one thread per kWilsonRows rows of one column from registers, 5 one
-// thread per 4-D column with warp-shuffled x neighbours (Nx a multiple of 32). Unless
+// thread per 4-D column with warp-shuffled x neighbours (Nx a multiple of 32); the
+// slice-ring kernel (6) is not a candidate (slower than 5 wherever measured). Unless
 // the context fixes the chunk length, the t sweep is timed at its automatic
 // shape and at chunks of 16, 32, 64 and 128 rows with the widest block and
 // with a half and a quarter of its 32-x tiles: long chunks amortise the ring's
@@ -856,7 +879,7 @@ int dwf_ctx_destroy(dwf_ctx* c)
     void* bufs[] = {c->h_mom, c->h_force, c->h_part, c->h_scal, c->h_chi, c->h_phi, c->h_eta,
                     c->h_xi, c->theta, c->U64, c->U32, c->w_r, c->w_p, c->w_p2, c->w_p32b, c->w_t, c->w_b, c->w_x,
                     c->w_r32, c->w_p32, c->w_t32, c->w_e32, c->w_src, c->w_part, c->w_conf, c->w_active,
-                    c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar,
+                    c->w_iters, c->w_relres, c->w_status, c->w_ru, c->w_true, c->bar, c->dslash_err,
                     c->eo_se, c->eo_so, c->eo_bh, c->eo_rhs_o, c->eo_x, c->eo_r, c->eo_t, c->eo_y,
                     c->eo_xn, c->eo_r32, c->eo_p32, c->eo_t32, c->eo_y32, c->eo_e32,
                     c->eo_phase, c->m_red, c->m_loop, c->m_z4};
@@ -968,6 +991,17 @@ int dwf_apply(dwf_ctx* c, int op, int conf, const double* in, double* out, int n
         return st;
     CK(cudaMemcpyAsync(out, c->w_x, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->dslash_err)
+    {
+        // a slice-ring Dslash wait that ran out (in this call or an earlier dwf_apply_dev)
+        int e = 0;
+        CK(cudaMemcpy(&e, c->dslash_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e != 0)
+        {
+            CK(cudaMemset(c->dslash_err, 0, sizeof(int)));
+            return ctx_fail(c, e, "apply: a slice-ring Dslash copy wait ran out");
+        }
+    }
     return DWF_OK;
 }
 
@@ -1061,8 +1095,15 @@ uint64_t dwf_launch_count(const dwf_ctx* c) { return c ? c->launches : 0; }
 
 int dwf_set_dslash_variant(dwf_ctx* c, int variant)
 {
-    if (!c || variant < -1 || variant > 5)
+    if (!c || variant < -1 || variant > 6)
         return DWF_BAD_ARG;
+    if (variant == 6 && !c->dslash_err)
+    {
+        // the slice-ring kernel's error word
+        CK(cudaSetDevice(c->device));
+        CK(cudaMalloc(&c->dslash_err, sizeof(int)));
+        CK(cudaMemset(c->dslash_err, 0, sizeof(int)));
+    }
     c->dslash_variant = variant;
     if (variant == -1)
         c->dslash_tuned.clear();

@@ -22,7 +22,7 @@ struct dwf_ctx
     uint64_t gauge_version = 0;  // bumped whenever the links change
     struct LpNet* lp = nullptr;  // learned preconditioner (dwf_lp_init)
     uint64_t launches = 0;  // kernels launched by this context
-    // Dslash kernel variant (-1 autotune, 0-4 as dwf_set_dslash_variant
+    // Dslash kernel variant (-1 autotune, 0-6 as dwf_set_dslash_variant
     // lists them); tuned choices cached per (precision, batch-size bucket),
     // for the t-sweeping kernel with its chunk length and 32-x tiles per block
     // (0: the automatic shape).
@@ -36,6 +36,7 @@ struct dwf_ctx
     int dslash_chunk = 0;    // rows per chunk of the t-sweeping Dslash (0 = automatic)
     int sweep_smem_set = 0;  // t-sweeping kernels whose shared-memory limit is raised (bits)
     int l1_pref_set = 0;     // shared-memory-free Dslash kernels asked for the largest L1 (bits)
+    int* dslash_err = nullptr;  // device word: DWF_TIMEOUT from a slice-ring Dslash wait (variant 6)
     std::map<int, DslashChoice> dslash_tuned;
     // CUDA events bracketing each persistent solver launch on `stream`
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -300,6 +300,225 @@ DWFB_COLX(false, float)
 DWFB_COLX(true, float)
 #undef DWFB_COLX
 
+// ---------------------------------------------------------------------------
+// Column kernel over a block-shared slice ring filled by bulk copies
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void tile_mbar_init(uint32_t mb, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mb), "r"(count));
+}
+
+__device__ __forceinline__ void tile_expect_tx(uint32_t mb, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes)
+                 : "memory");
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, completing on mbarrier mb
+// (both addresses 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void tile_bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mb)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(mb)
+        : "memory");
+}
+
+// Wait for the phase of parity `par` of mbarrier mb; false once limit_ns has
+// passed (the timer is read every 64 polls).
+__device__ __forceinline__ bool tile_wait(uint32_t mb, uint32_t par, unsigned long long limit_ns)
+{
+    unsigned long long t0 = 0;
+    for (int it = 0;; ++it)
+    {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mb), "r"(par)
+            : "memory");
+        if (done)
+            return true;
+        if ((it & 63) == 0)
+        {
+            const unsigned long long t = globaltimer_ns();
+            if (it == 0)
+                t0 = t;
+            else if (t - t0 > limit_ns)
+                return false;
+        }
+    }
+}
+
+template <bool DAG, typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? DWFB_TILE_MINB64 : DWFB_TILE_MINB32)
+    dirac_tile_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out, long fsz,
+                      const cplx<R>* __restrict__ U, long usz, const int* __restrict__ conf,
+                      int conf0, int* err, unsigned long long limit_ns)
+{
+    using T = cplx<R>;
+    constexpr int NS = kRingSlots, NW = kRingT;
+    constexpr uint32_t SB = 2 * sizeof(T);           // bytes of one site's spinor
+    constexpr int kSlot = kRingRows * kRingWidth;    // sites per ring slot
+    constexpr int kPrev = DAG ? 1 : 0, kNext = DAG ? 0 : 1;
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    const T* ring = reinterpret_cast<const T*>(tile_smem);
+    const uint32_t ring0 = uint32_t(__cvta_generic_to_shared(tile_smem));
+    // after the ring: full[k][w] (warp w's rows of slot k landed), empty[k]
+    // (all warps done with slot k)
+    const uint32_t full0 = ring0 + NS * kSlot * SB;
+    const uint32_t empty0 = full0 + 8 * NS * NW;
+
+    const int j = blockIdx.z;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int Nt = L.Nt, Nx = L.Nx, V = L.V, Ls = L.Ls;
+    const int x0 = blockIdx.x * 32, t0 = blockIdx.y * NW;
+    const int t = t0 + warp, x = x0 + lane;
+    const int c = conf ? conf[j] : conf0;
+    const T* __restrict__ Uj = U + long(c) * usz;
+    const T* __restrict__ inj = in + j * fsz;
+    T* __restrict__ outj = out + j * fsz;
+
+    if (threadIdx.x == 0)
+    {
+        for (int k = 0; k < NS * NW; ++k)
+            tile_mbar_init(full0 + 8 * k, 1);
+        for (int k = 0; k < NS; ++k)
+            tile_mbar_init(empty0 + 8 * k, NW);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // Warp w copies ring row w + 1 (its own t row) of each slice, warp 0 also
+    // row 0 (t0 - 1) and warp NW - 1 row NW + 1 (t0 + NW): per row, lane 3i
+    // the sites x0 - 1 .. x0 + 32 that do not cross the x boundary, lanes
+    // 3i + 1 and 3i + 2 the one site on either side that does (periodic in t and x).
+    const int row_a = (warp == 0) ? 0 : warp + 1;
+    const int nrows = (warp == 0 || warp == NW - 1) ? 2 : 1;
+    auto issue = [&](int s) {
+        const int k = s % NS;
+        const uint32_t mb = full0 + 8 * (k * NW + warp);
+        if (lane == 0)
+            tile_expect_tx(mb, uint32_t(nrows * kRingWidth) * SB);
+        __syncwarp();
+        if (lane < 3 * nrows)
+        {
+            const int r = row_a + lane / 3, part = lane % 3;
+            int tr = t0 - 1 + r;
+            tr = tr < 0 ? tr + Nt : (tr >= Nt ? tr - Nt : tr);
+            const T* row = inj + 2 * (long(s) * V + long(tr) * Nx);
+            const uint32_t dst = ring0 + uint32_t(k * kSlot + r * kRingWidth) * SB;
+            const int lo = (x0 == 0) ? 1 : 0, hi = (x0 + 32 == Nx) ? kRingWidth - 1 : kRingWidth;
+            if (part == 0)
+                tile_bulk_g2s(dst + lo * SB, row + 2 * (x0 - 1 + lo), uint32_t(hi - lo) * SB, mb);
+            else if (part == 1 && lo)
+                tile_bulk_g2s(dst, row + 2 * (Nx - 1), SB, mb);
+            else if (part == 2 && hi < kRingWidth)
+                tile_bulk_g2s(dst + (kRingWidth - 1) * SB, row, SB, mb);
+        }
+    };
+    for (int s = 0; s < NS && s < Ls; ++s)
+        issue(s);
+    int issued = NS < Ls ? NS : Ls;  // slices 0 .. issued - 1 copied or in flight
+
+    // link phases with the boundary signs folded in
+    const int tm = (t == 0) ? Nt - 1 : t - 1;
+    const int xm = (x == 0) ? Nx - 1 : x - 1;
+    const int here = t * Nx + x;
+    const T Ut = ((t == Nt - 1) ? R(L.bct) : R(1)) * Uj[here];
+    const T Utm = ((t == 0) ? R(L.bct) : R(1)) * Uj[tm * Nx + x];
+    const T Ux = ((x == Nx - 1) ? R(L.bcx) : R(1)) * Uj[V + here];
+    const T Uxm = ((x == 0) ? R(L.bcx) : R(1)) * Uj[V + t * Nx + xm];
+    const R dg = R(L.diag), mf = R(L.mf);
+    T pv = {}, first_c = {};
+    if (L.fifth)
+        pv = inj[2 * (long(Ls - 1) * V + here) + kPrev];
+    const int rc = (warp + 1) * kRingWidth + lane + 1;  // this site in a slot
+    // the warps whose rows this warp reads: rows warp .. warp + 2 of a slot
+    const int w_lo = warp > 0 ? warp - 1 : 0, w_hi = warp < NW - 1 ? warp + 1 : NW - 1;
+
+    int s = 0;
+    for (; s < Ls; ++s)
+    {
+        const int k = s % NS;
+        const uint32_t par = (s / NS) & 1;
+        bool ok = tile_wait(full0 + 8 * (k * NW + w_lo), par, limit_ns) &&
+                  tile_wait(full0 + 8 * (k * NW + warp), par, limit_ns) &&
+                  tile_wait(full0 + 8 * (k * NW + w_hi), par, limit_ns);
+        if (ok && L.fifth && s + 1 < Ls)
+            ok = tile_wait(full0 + 8 * (((s + 1) % NS) * NW + warp), ((s + 1) / NS) & 1, limit_ns);
+        if (!__all_sync(0xffffffffu, ok))
+            break;
+        const T* S = ring + 2 * k * kSlot;
+        const Spinor<R> cur = ld_spinor(S, rc);
+        const Spinor<R> vtp = ld_spinor(S, rc + kRingWidth);
+        const Spinor<R> vtm = ld_spinor(S, rc - kRingWidth);
+        const Spinor<R> vxp = ld_spinor(S, rc + 1);
+        const Spinor<R> vxm = ld_spinor(S, rc - 1);
+        T up, lo;
+        hop4<DAG, R>(vtp, vtm, vxp, vxm, Ut, Utm, Ux, Uxm, R(1), R(1), R(1), R(1), up, lo);
+        Spinor<R> o{dg * cur.s0 - R(0.5) * up, dg * cur.s1 - R(0.5) * lo};
+        if (L.fifth)
+        {
+            if (s == 0)
+                first_c = kNext ? cur.s1 : cur.s0;
+            const R cup = (s + 1 == Ls) ? mf : R(-1);
+            const R cdn = (s == 0) ? mf : R(-1);
+            const T nc = (s + 1 < Ls) ? ring[2 * (((s + 1) % NS) * kSlot + rc) + kNext] : first_c;
+            if (!DAG)
+            {
+                o.s1 += cup * nc;
+                o.s0 += cdn * pv;
+            }
+            else
+            {
+                o.s1 += cdn * pv;
+                o.s0 += cup * nc;
+            }
+            pv = kPrev ? cur.s1 : cur.s0;
+        }
+        st_spinor(outj, long(s) * V + here, o);
+        // this warp is done with slot k (its slice s + 1 component was read at step s)
+        __syncwarp();
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(empty0 + 8 * k) : "memory");
+        // refill the slot freed at the previous step once every warp is done with it
+        if (s >= 1 && issued < Ls)
+        {
+            const int q = s - 1;
+            const bool free = tile_wait(empty0 + 8 * (q % NS), (q / NS) & 1, limit_ns);
+            if (!__all_sync(0xffffffffu, free))
+                break;
+            issue(issued);
+            ++issued;
+        }
+    }
+    if (s < Ls)
+    {
+        // a wait ran out: record it, and let this warp's copies in flight
+        // (slices s .. issued - 1) land before it exits (allowing them at
+        // least a second, however short the caller's limit)
+        if (lane == 0)
+        {
+            atomicCAS(err, 0, int(DWF_TIMEOUT));
+            const unsigned long long drain = limit_ns > 1000000000ull ? limit_ns : 1000000000ull;
+            for (int q = s; q < issued; ++q)
+                tile_wait(full0 + 8 * ((q % NS) * NW + warp), (q / NS) & 1, drain);
+        }
+    }
+}
+
+#define DWFB_TILE(DAG, R)                                                                          \
+    template __global__ void dirac_tile_kernel<DAG, R>(Lat, const cplx<R>*, cplx<R>*, long,         \
+                                                       const cplx<R>*, long, const int*, int, int*, \
+                                                       unsigned long long);
+DWFB_TILE(false, double)
+DWFB_TILE(true, double)
+DWFB_TILE(false, float)
+DWFB_TILE(true, float)
+#undef DWFB_TILE
+
 template __global__ void dirac_col_kernel<false, double>(Lat, const double2*, double2*, long,
                                                          const double2*, long, const int*, int);
 template __global__ void dirac_col_kernel<true, double>(Lat, const double2*, double2*, long,

@@ -33,6 +33,38 @@ __global__ void dirac_colx_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>
                                   long fsz, const cplx<R>* __restrict__ U, long usz,
                                   const int* __restrict__ conf, int conf0);
 
+// Same operator over a block-shared ring of kRingSlots slices in shared
+// memory, filled by 1-D bulk copies (cp.async.bulk, mbarrier completion): a
+// block of 8 warps covers 32 x by kRingT t rows and sweeps s; warp 0 copies
+// each slice's kRingRows x kRingWidth sites (the tile and its halo) kRingSlots
+// slices ahead, every neighbour is read from shared memory, and a block
+// barrier per slice frees the slot for the next copy (Nx % 32 == 0,
+// Nt % kRingT == 0; grid Nx/32 x Nt/kRingT x nrhs, 256 threads, dynamic
+// shared memory tile_smem_bytes). Warp w copies its own t row (warps 0 and
+// 7 also the halo rows), signals an mbarrier of its own per slot, and refills
+// a slot once all eight warps have arrived on the slot's release barrier. A
+// wait longer than limit_ns sets *err to DWF_TIMEOUT and ends the warp once
+// its own copies have landed.
+#ifndef DWFB_RING_SLOTS
+#define DWFB_RING_SLOTS 4
+#endif
+constexpr int kRingT = 8, kRingRows = kRingT + 2, kRingWidth = 34, kRingSlots = DWFB_RING_SLOTS;
+#ifndef DWFB_TILE_MINB64
+#define DWFB_TILE_MINB64 4  // resident blocks per SM asked of the FP64 build
+#endif
+#ifndef DWFB_TILE_MINB32
+#define DWFB_TILE_MINB32 4
+#endif
+__host__ __device__ constexpr size_t tile_smem_bytes(size_t site_bytes)
+{
+    return size_t(kRingSlots) * kRingRows * kRingWidth * site_bytes + 8 * kRingSlots * (kRingT + 1);
+}
+template <bool DAG, typename R>
+__global__ void dirac_tile_kernel(Lat L, const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                                  long fsz, const cplx<R>* __restrict__ U, long usz,
+                                  const int* __restrict__ conf, int conf0, int* err,
+                                  unsigned long long limit_ns);
+
 // Wilson only (Ls = 1, no fifth dimension; Nx % 32 == 0, Nt % RT == 0): a
 // warp covers 32 consecutive x of RT consecutive rows, each thread loading
 // its column's rows t0-1 .. t0+RT into registers up front (RT + 2 spinor loads

@@ -170,7 +170,12 @@ int dwf_cg_batch(dwf_ctx* ctx, int op, int nrhs, const int* rhs_conf, const doub
 /* The analyzers' propagator solve for nrhs sources at once: x = (D^dag D)^-1 D^dag src,
  * i.e. rhs = apply_D_dagger(theta, source) followed by conjugate_gradient on
  * apply_D_dagger_D from zero (domain_wall/include/correlator.hpp:77-79, :139-142,
- * :213-220). info[k].dirac_relres = |D x - src| / |src|. Host buffers. */
+ * :213-220). info[k].dirac_relres = |D x - src| / |src|. Host buffers. With
+ * DWF_SOLVER_EO_MIXED on the cluster solver and nrhs of at least two of its
+ * waves (the right-hand sides its resident clusters solve at once), the batch
+ * runs in two chunks of whole waves, the copies of each chunk on a second
+ * stream overlapping the solve of the other (page-locked buffers let them
+ * overlap); every right-hand side is solved as in one batch. */
 int dwf_propagators(dwf_ctx* ctx, int nrhs, const int* rhs_conf, const double* src, double* x,
                     double rtol, int maxiter, int solver, dwf_solve_info* info);
 /* Device-buffer version. */

@@ -17,6 +17,10 @@ struct dwf_ctx
     int device = 0;
     int nsm = 0;
     cudaStream_t stream = nullptr;
+    // host-buffer propagator batches: copies on a second stream, overlapped
+    // with the solve of the neighbouring chunks (created on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pipe_ev[8] = {};
     uint64_t timeout_ns = 5000000000ull;
     std::string err;
     uint64_t gauge_version = 0;  // bumped whenever the links change
@@ -157,6 +161,9 @@ int set_gauge(dwf_ctx* c, int nconf, const double* theta, cudaMemcpyKind kind);
 int propagators_eo(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
                    double tol, int maxiter, std::vector<int>& iters, std::vector<int>& ru);
 bool eo_eligible(const dwf_ctx* c);
+// Right-hand sides the even-odd cluster solver runs at once on this context's
+// lattice and device (its resident clusters), 0 where the cluster path does not apply.
+int eo_cluster_wave(dwf_ctx* c);
 // Propagator batch: x = (D^dag D)^-1 D^dag src on device fields.
 int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, double2* x,
                 double rtol, int maxiter, int solver, dwf_solve_info* info);

@@ -33,7 +33,7 @@ __global__ void eo_combine_kernel(Lat L, EoGeo g, const double2* a, const double
                                   const double2* y, double2* out, const double2* U, long usz,
                                   const int* conf, long nrhs);
 __global__ void cg_eo_mixed_kernel(EoDesc e);
-int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched, bool dry);
+int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched, bool dry, int* wave = nullptr);
 
 // DWF_B200_EO_KERNEL=grid keeps every even-odd solve on the grid-wide kernel
 // (cg_eo_mixed_kernel); by default the cluster kernel (eo_cluster.cu) takes
@@ -50,6 +50,20 @@ bool eo_cluster_enabled()
 bool eo_eligible(const dwf_ctx* c)
 {
     return c->kind == 0 && c->L.Nt % 2 == 0 && c->L.Nx % 2 == 0 && c->L.diag >= 1.0;
+}
+
+int eo_cluster_wave(dwf_ctx* c)
+{
+    if (!eo_eligible(c) || c->eo_kernel == 0 || !eo_cluster_enabled())
+        return 0;
+    EoDesc e{};
+    e.d.nrhs = 1;
+    e.d.delta = 0.1;
+    bool ok = false;
+    int wave = 0;
+    if (launch_eo_cluster(c, e, &ok, true, &wave) != DWF_OK || !ok)
+        return 0;
+    return wave;
 }
 
 namespace {

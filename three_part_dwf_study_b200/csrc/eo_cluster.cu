@@ -746,7 +746,8 @@ DWFB_CL_SHAPES(DWFB_CL_INST)
 // Launch the cluster solver for a batch prepared by propagators_eo (fields in
 // EoDesc as for cg_eo_mixed_kernel). Returns DWF_BAD_ARG (nothing launched)
 // when the lattice or the device does not allow it: the caller then runs the
-// grid-wide kernel.
+// grid-wide kernel. A dry call only checks, and reports in *wave (when not
+// null) how many right-hand sides the resident clusters solve at once.
 // Launch shape of the cluster kernel per (device, kernel): attributes set and
 // the resident-cluster count queried once, so that a later call (the one a
 // stream capture records) issues the launch alone.
@@ -757,7 +758,7 @@ struct ClLaunchShape
 
 // dry: check that the cluster kernel takes this batch and prepare its launch
 // shape without launching (*launched tells whether it would launch).
-int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched, bool dry)
+int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched, bool dry, int* wave)
 {
     static std::map<std::pair<int, const void*>, ClLaunchShape> shapes;
     static std::mutex shapes_mu;
@@ -849,6 +850,8 @@ int launch_eo_cluster(dwf_ctx* c, EoDesc& e, bool* launched, bool dry)
     if (dry)
     {
         *launched = true;
+        if (wave)
+            *wave = sh.nclust;
         return DWF_OK;
     }
     const int nclust = std::min(sh.nclust, e.d.nrhs);

@@ -23,9 +23,12 @@ using namespace dwfb;
 // 4 / 3 -> 829, 4 / 4 -> 788, 4 / 6 -> 735, 2 / 3 -> 828, 2 / 4 -> 786.
 // The full-lattice solve now runs only when the FP64 residual of the full
 // normal equation misses the tolerance after the Schur solve; with the
-// cluster Schur kernel (GPU-HMC configuration, factor: solves/s): 3 -> 1252
-// (the check fails and the full-lattice solve runs), 1 -> 1311 (it passes),
-// 0.5 -> 1267, 0.3 -> 1265.
+// cluster Schur kernel (GPU-HMC configuration, factor: solves/s): 3 -> 1252,
+// 1 -> 1311, 0.5 -> 1267, 0.3 -> 1265; on three configurations of the chain
+// 1 -> 1311 / 1339 / 1329, 0.85 -> 1306 / 1329 / 1314, 0.7 -> 1293 / 1324 / 1293.
+// At 0.7 - 3 the check still misses by a little and the full-lattice solve adds
+// at most 4 iterations per source (about 0.6 ms per 28-source batch), which costs
+// less than the Schur iterations that would make the check pass.
 #ifndef DWFB_EO_SCHUR_TOL
 #define DWFB_EO_SCHUR_TOL 1.0
 #endif

@@ -71,8 +71,9 @@ typedef enum
     DWF_SOLVER_MIXED = 1,
     /* Propagator solves (dwf_propagators, dwf_measure): even-odd
      * (4-D checkerboard) Schur-complement preconditioned mixed CG for
-     * D x = src, then DWF_SOLVER_MIXED on the full D^dag D from that x, so the
-     * reference's stopping rule on the full normal equation decides. Needs even
+     * D x = src, then, where the FP64 residual of the full D^dag D misses rtol,
+     * DWF_SOLVER_CG64 on the full D^dag D from that x, so the reference's
+     * stopping rule on the full normal equation decides. Needs even
      * Nt, Nx and 3 - M5 >= 1 (else it runs DWF_SOLVER_MIXED); elsewhere it is
      * DWF_SOLVER_MIXED. */
     DWF_SOLVER_EO_MIXED = 2,

@@ -1,9 +1,9 @@
 """Even-odd (Schur-complement) preconditioned propagator solves on the GPU.
 
 The even-odd stage solves Dhat x_o = b_o - H_oe M5^-1 b_e on the odd sites and
-reconstructs x_e; the full-lattice mixed solve that follows enforces the
+reconstructs x_e; the full-lattice FP64 solve that follows enforces the
 reference's stopping rule on D^dag D. Checked: the stage does nearly all the
-work (the full-lattice check needs at most two reliable-update periods), the
+work (the full-lattice check needs a few iterations at most), the
 result equals the FP64 reference-algorithm solution, the analyzer outputs
 match the reference's golden vectors, and lattices the stage cannot take fall
 back."""

@@ -26,11 +26,18 @@ using namespace dwfb;
 // cluster Schur kernel (GPU-HMC configuration, factor: solves/s): 3 -> 1252,
 // 1 -> 1311, 0.5 -> 1267, 0.3 -> 1265; on three configurations of the chain
 // 1 -> 1311 / 1339 / 1329, 0.85 -> 1306 / 1329 / 1314, 0.7 -> 1293 / 1324 / 1293.
-// At 0.7 - 3 the check still misses by a little and the full-lattice solve adds
-// at most 4 iterations per source (about 0.6 ms per 28-source batch), which costs
-// less than the Schur iterations that would make the check pass.
+// At 0.7 - 3 the check still misses by a little and the full-lattice mixed
+// solve adds at most 4 iterations per source (about 0.6 ms per 28-source batch).
+// The full-lattice solve in FP64 (DWFB_EO_POLISH_SOLVER) checks the true residual
+// every iteration where the warm-started mixed one waits for its first reliable
+// update: 2-3 iterations, and a looser Schur stop then pays (three
+// configurations, solves/s): mixed, factor 1 -> 1313 / 1346 / 1334; FP64, 1 ->
+// 1331 / 1365 / 1354; 1.5 -> 1368 / 1387 / 1364; 2 -> 1385 / 1403 / 1377.
 #ifndef DWFB_EO_SCHUR_TOL
-#define DWFB_EO_SCHUR_TOL 1.0
+#define DWFB_EO_SCHUR_TOL 2.0
+#endif
+#ifndef DWFB_EO_POLISH_SOLVER
+#define DWFB_EO_POLISH_SOLVER DWF_SOLVER_CG64
 #endif
 #ifndef DWFB_PIPE_CHUNKS
 // Chunks of a host-buffer even-odd cluster batch (1 to 4). At 64x64x16 with 28
@@ -735,7 +742,7 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
     if (solver == DWF_SOLVER_EO_MIXED && eo_eligible(c))
     {
         // Even-odd Schur solve of D x = src as the starting point, then the
-        // full-lattice mixed solve on D^dag D from it: the reference's
+        // full-lattice solve on D^dag D from it: the reference's
         // stopping rule |D^dag D x - D^dag src| <= rtol |D^dag src| decides.
         std::vector<int> eo_it, eo_ru;
         st = propagators_eo(c, nrhs, conf_h, src, x, DWFB_EO_SCHUR_TOL * rtol, maxiter, eo_it, eo_ru);
@@ -773,9 +780,9 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
         }
         else
         {
-            // the full-lattice mixed solve on D^dag D from the even-odd solution
+            // the full-lattice solve on D^dag D from the even-odd solution
             st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 1, rtol, maxiter,
-                             DWF_SOLVER_MIXED, 0, info);
+                             DWFB_EO_POLISH_SOLVER, 0, info);
             if (st)
                 return st;
             for (int k = 0; info && k < nrhs; ++k)

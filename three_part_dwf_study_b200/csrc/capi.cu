@@ -32,7 +32,10 @@ using namespace dwfb;
 // every iteration where the warm-started mixed one waits for its first reliable
 // update: 2-3 iterations, and a looser Schur stop then pays (three
 // configurations, solves/s): mixed, factor 1 -> 1313 / 1346 / 1334; FP64, 1 ->
-// 1331 / 1365 / 1354; 1.5 -> 1368 / 1387 / 1364; 2 -> 1385 / 1403 / 1377.
+// 1331 / 1365 / 1354; 1.5 -> 1368 / 1387 / 1364; 2 -> 1385 / 1403 / 1377; 3 ->
+// 1404 / 1401 / 1393 (up to 5 iterations); 4 -> 1127 / 1150 / 1142 (up to 67:
+// past about 3x the full-lattice solve has to remove the Schur solution's low
+// modes). 2 keeps a margin below that edge.
 #ifndef DWFB_EO_SCHUR_TOL
 #define DWFB_EO_SCHUR_TOL 2.0
 #endif

@@ -176,7 +176,8 @@ int dwf_cg_batch(dwf_ctx* ctx, int op, int nrhs, const int* rhs_conf, const doub
  * waves (the right-hand sides its resident clusters solve at once), the batch
  * runs in two chunks of whole waves, the copies of each chunk on a second
  * stream overlapping the solve of the other (page-locked buffers let them
- * overlap); every right-hand side is solved as in one batch. */
+ * overlap); each source's Schur solve is the one a single batch would run,
+ * and the full-lattice check is decided per chunk. */
 int dwf_propagators(dwf_ctx* ctx, int nrhs, const int* rhs_conf, const double* src, double* x,
                     double rtol, int maxiter, int solver, dwf_solve_info* info);
 /* Device-buffer version. */

@@ -1169,7 +1169,8 @@ int dwf_propagators(dwf_ctx* c, int nrhs, const int* rhs_conf, const double* src
     // chunks of whole waves, the sources of every chunk copied in and the
     // solutions of each finished chunk copied out on a second stream while
     // the next chunks solve (the copies overlap the solves when the host
-    // buffers are page-locked). Each right-hand side is solved as in one batch.
+    // buffers are page-locked). Each right-hand side's Schur solve is the one
+    // a single batch would run; the full-lattice check is decided per chunk.
     const int wave = solver == DWF_SOLVER_EO_MIXED ? eo_cluster_wave(c) : 0;
     if (wave > 0 && nrhs >= 2 * wave)
         return propagators_pipelined(c, nrhs, rhs_conf, src, x, rtol, maxiter, solver, info,

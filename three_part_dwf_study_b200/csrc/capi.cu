@@ -35,12 +35,22 @@ using namespace dwfb;
 // 1331 / 1365 / 1354; 1.5 -> 1368 / 1387 / 1364; 2 -> 1385 / 1403 / 1377; 3 ->
 // 1404 / 1401 / 1393 (up to 5 iterations); 4 -> 1127 / 1150 / 1142 (up to 67:
 // past about 3x the full-lattice solve has to remove the Schur solution's low
-// modes). 2 keeps a margin below that edge.
+// modes). 2 keeps a margin below that edge. Where the grid-wide Schur kernel
+// runs (right-hand sides too large for a cluster) the same pair cost the
+// finite-volume study at 64x96x16 (1792 sources) 20 % (451.5 against 561.9
+// solves/s; 64x80x16: 719.6 against 706.5), so that path keeps factor 1 and
+// the mixed check solve.
 #ifndef DWFB_EO_SCHUR_TOL
-#define DWFB_EO_SCHUR_TOL 2.0
+#define DWFB_EO_SCHUR_TOL 2.0       // cluster Schur kernel
 #endif
 #ifndef DWFB_EO_POLISH_SOLVER
 #define DWFB_EO_POLISH_SOLVER DWF_SOLVER_CG64
+#endif
+#ifndef DWFB_EO_SCHUR_TOL_GRID
+#define DWFB_EO_SCHUR_TOL_GRID 1.0  // grid-wide Schur kernel
+#endif
+#ifndef DWFB_EO_POLISH_SOLVER_GRID
+#define DWFB_EO_POLISH_SOLVER_GRID DWF_SOLVER_MIXED
 #endif
 #ifndef DWFB_PIPE_CHUNKS
 // Chunks of a host-buffer even-odd cluster batch (1 to 4). At 64x64x16 with 28
@@ -748,7 +758,9 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
         // full-lattice solve on D^dag D from it: the reference's
         // stopping rule |D^dag D x - D^dag src| <= rtol |D^dag src| decides.
         std::vector<int> eo_it, eo_ru;
-        st = propagators_eo(c, nrhs, conf_h, src, x, DWFB_EO_SCHUR_TOL * rtol, maxiter, eo_it, eo_ru);
+        const bool clustered = eo_cluster_wave(c) > 0;
+        const double schur_tol = (clustered ? DWFB_EO_SCHUR_TOL : DWFB_EO_SCHUR_TOL_GRID) * rtol;
+        st = propagators_eo(c, nrhs, conf_h, src, x, schur_tol, maxiter, eo_it, eo_ru);
         if (st)
             return st;
         // The reference's rule on the full normal equation, in FP64: where every
@@ -785,7 +797,7 @@ int propagators(dwf_ctx* c, int nrhs, const int* conf_h, const double2* src, dou
         {
             // the full-lattice solve on D^dag D from the even-odd solution
             st = solve_batch(c, DWF_OP_DDAGD, nrhs, conf_h, c->w_b, x, 1, rtol, maxiter,
-                             DWFB_EO_POLISH_SOLVER, 0, info);
+                             clustered ? DWFB_EO_POLISH_SOLVER : DWFB_EO_POLISH_SOLVER_GRID, 0, info);
             if (st)
                 return st;
             for (int k = 0; info && k < nrhs; ++k)
